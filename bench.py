@@ -1,0 +1,406 @@
+"""Benchmark: batched FFA search of DM trials (ffa_search = deredden + normalise + periodogram)
+on B200, against the reference's CPU implementation.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config 3]
+
+One step = one search of the whole synthetic batch (default: 512 trials of
+U[0.9, 1.0] * 2^22 samples, 64 us, P 0.2-30 s, bins 240-260). Prints one JSON line on rank 0.
+Under torchrun each rank searches its own batch (weak scaling, no data-path collective).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = ("DM-trial searches/s (2^22 samp, 0.2–60 s) batched vs plain GPU at equal S/N; "
+          "%HBM")
+FALLBACK_HBM_GBS = 6650.0
+
+
+# --------------------------------------------------------------------------------------
+# CPU reference arm (runs in spawned worker processes)
+# --------------------------------------------------------------------------------------
+def _cpu_worker(args):
+    data, tsamp, kw = args
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    sys.path.insert(0, HERE)
+    from oracle import oracle as O
+
+    ref = O.ref_libcpp()
+    t0 = time.perf_counter()
+    O.ffa_search(data, tsamp, libcpp=ref, **kw)
+    return time.perf_counter() - t0
+
+
+def cpu_kind():
+    from oracle import oracle as O
+
+    return "reference" if O.ref_libcpp() is not None else "port"
+
+
+def cpu_sample_trials(config_id, nsample, first_index=1_000_000):
+    """Host copies of `nsample` synthetic trials (generated on the GPU, same generator)."""
+    from riptide_b200 import synth
+
+    cfg = synth.CONFIGS[config_id]
+    lengths = synth.trial_lengths(config_id, nsample, first_index)
+    out = []
+    for k, n in enumerate(lengths):
+        x, _ = synth.make_trial(config_id, first_index + k, n, cfg["tsamp"], "cuda")
+        out.append(x.cpu().numpy())
+    return out
+
+
+def run_cpu_steps(pool, trials, tsamp, kw, steps):
+    """Time `steps` rounds; each round searches every trial of the sample in parallel."""
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        list(pool.map(_cpu_worker, [(x, tsamp, kw) for x in trials]))
+        times.append(time.perf_counter() - t0)
+    return times
+
+
+def cpu_pool(ncores):
+    import multiprocessing as mp
+
+    return mp.get_context("spawn").Pool(processes=ncores)
+
+
+# --------------------------------------------------------------------------------------
+# helpers
+# --------------------------------------------------------------------------------------
+class ClockSampler(object):
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while active."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [v.strip() for v in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_per_trial():
+    """DRAM bytes per trial of the search kernel from the committed ncu summary, or None."""
+    try:
+        with open(os.path.join(HERE, "profiles", "search_persistent_traffic.json")) as f:
+            return float(json.load(f)["dram_bytes_per_trial"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# --------------------------------------------------------------------------------------
+def bench_reference(args):
+    """--impl reference: the reference's CPU implementation on the host cores."""
+    world, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return 0
+    from riptide_b200 import synth
+
+    cfg = synth.CONFIGS[args.config]
+    ncores = os.cpu_count() or 1
+    nsample = max(1, min(ncores, args.cpu_sample))
+    trials = cpu_sample_trials(args.config, nsample)
+    kw = dict(cfg["search"])
+    pool = cpu_pool(ncores)
+    try:
+        run_cpu_steps(pool, trials, cfg["tsamp"], kw, args.warmup and 1)
+        times = run_cpu_steps(pool, trials, cfg["tsamp"], kw, args.steps)
+    finally:
+        pool.close()
+    step = float(np.mean(times))
+    value = nsample / step
+    kind = cpu_kind()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "trials/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": cfg["name"], "trials_per_step": nsample},
+        "cpu_baseline": {"value": value, "unit": "trials/s", "cores": ncores, "kind": kind,
+                         "sample": f"{nsample} trials of the workload per step, one per process"},
+        "e2e": {"value": value, "unit": "trials/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def bench_ours(args):
+    world, rank, local = dist_setup()
+    import torch
+
+    import riptide_b200 as rb
+    from riptide_b200 import synth
+
+    torch.cuda.set_device(local)
+    cfg = synth.CONFIGS[args.config]
+    ntrials = args.trials
+    # CPU baseline pool is spawned before any heavy GPU work of this process
+    ncores = os.cpu_count() or 1
+    do_cpu = (rank == 0 and world == 1 and not args.no_cpu)
+    pool = cpu_pool(ncores) if do_cpu else None
+
+    data, lengths, infos = synth.make_batch(args.config, ntrials, first_index=rank * ntrials)
+    t0 = time.perf_counter()
+    bs = rb.BatchedSearch(lengths, cfg["tsamp"], **cfg["search"])
+    plan_ms = (time.perf_counter() - t0) * 1e3
+    st = bs.stats
+    nw = int(bs.widths.size)
+    L = st["total_rows"]
+    bytes_kernel = 4 * st["folded_samples"] + L * (4 * nw + 12)
+    bytes_job = 4 * st["total_samples"] + 4 * st["downsampled_samples"] + bytes_kernel
+
+    outs = bs.allocate_outputs()
+    bs.run(data, outs, check=True)  # first run allocates the plan's device buffers
+    for _ in range(max(0, args.warmup - 1)):
+        bs.run(data, outs, check=False)
+    torch.cuda.synchronize()
+    bs.enable_timing(True)
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stage = np.zeros(3)
+    launches = 0
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            bs.run(data, outs, check=False)
+            s0, s1, s2, n = bs.last_timing()
+            stage += (s0, s1, s2)
+            launches += n
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    bs.enable_timing(False)
+    from riptide_b200 import _lib
+
+    _lib.check(_lib.load().rt_search_check(bs._plan, _lib.ctypes.c_void_p(stream.cuda_stream)))
+    ms = e0.elapsed_time(e1) / args.steps
+    ms = max_over_ranks(ms, world)
+    value = ntrials * world / (ms * 1e-3)
+    k_ms = stage[2] / args.steps
+    peak, peak_kind = measured_peak()
+    achieved = bytes_kernel / (k_ms * 1e-3) / 1e9
+    tr = traffic_per_trial()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": (tr * ntrials if tr else None),
+                "kernel": "k_search_persistent", "peak_source": peak_kind,
+                "alg_bytes_per_launch": bytes_kernel}
+
+    # ---- end to end through the public API with host buffers (rank 0 prints) ----
+    e2e = None
+    if not args.no_e2e:
+        host_in = data.cpu().pin_memory()
+        host_out = [torch.empty(o.shape, dtype=o.dtype, pin_memory=True) for o in outs]
+        dev_in = torch.empty_like(data)
+        h2d = host_in.numel() * 4
+        d2h = sum(o.numel() * o.element_size() for o in outs)
+        def e2e_step():
+            dev_in.copy_(host_in, non_blocking=True)
+            bs.run(dev_in, outs, check=False)
+            for h, o in zip(host_out, outs):
+                h.copy_(o, non_blocking=True)
+        e2e_step()
+        torch.cuda.synchronize()
+        barrier(world)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(max(1, args.e2e_steps)):
+            e2e_step()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ems = max_over_ranks(a.elapsed_time(b) / max(1, args.e2e_steps), world)
+        e2e = {"value": ntrials * world / (ems * 1e-3), "unit": "trials/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "ms_per_step": ems}
+        del host_in, host_out, dev_in
+
+    # ---- plain per-(cycle, bins) GPU path on a few trials, for the batching ratio ----
+    plain = None
+    if rank == 0 and args.plain_trials > 0:
+        offs = np.concatenate([[0], np.cumsum(lengths)])
+        tms = []
+        for i in range(args.plain_trials):
+            x = data[int(offs[i]):int(offs[i + 1])]
+            t1 = time.perf_counter()
+            y = torch.empty_like(x)
+            z = torch.empty_like(x)
+            p = rb.libcpp
+            _lib.check(_lib.load().rt_deredden(p._ptr(x), x.numel(), cfg["tsamp"],
+                                               cfg["search"]["rmed_width"],
+                                               cfg["search"]["rmed_minpts"], p._ptr(y), p._stream()))
+            _lib.check(_lib.load().rt_normalise(p._ptr(y), y.numel(), p._ptr(z), p._stream()))
+            rb.libcpp.periodogram_plain(z, cfg["tsamp"], bs.widths, cfg["search"]["period_min"],
+                                        cfg["search"]["period_max"], cfg["search"]["bins_min"],
+                                        cfg["search"]["bins_max"])
+            torch.cuda.synchronize()
+            tms.append(time.perf_counter() - t1)
+        plain = {"trials_per_s": 1.0 / float(np.median(tms)), "sample_trials": args.plain_trials}
+
+    # ---- CPU baseline (rank 0, N = 1) ----
+    cpu = None
+    if do_cpu:
+        nsample = max(1, min(ncores, args.cpu_sample))
+        trials = cpu_sample_trials(args.config, nsample)
+        run_cpu_steps(pool, trials[:1], cfg["tsamp"], dict(cfg["search"]), 1)
+        times = run_cpu_steps(pool, trials, cfg["tsamp"], dict(cfg["search"]), 1)
+        pool.close()
+        cpu = {"value": nsample / times[0], "unit": "trials/s", "cores": ncores,
+               "kind": cpu_kind(),
+               "sample": f"{nsample} trials of the workload searched in parallel, one per process"}
+
+    if rank == 0:
+        clocks = clk.summary()
+        line = {
+            "metric": METRIC, "value": value, "unit": "trials/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded white + 1/f noise + von Mises pulsars, generated on device)",
+            "config": {"workload": cfg["name"], "trials_per_gpu": ntrials,
+                       "samples_per_gpu": int(sum(lengths)), "periodogram_rows_per_gpu": L,
+                       "widths": nw, "l2": "inputs larger than L2 (%.1f GB per step)" %
+                       (4 * sum(lengths) / 1e9),
+                       "plan_ms": plan_ms, "stage_ms": {"deredden_normalise": stage[0] / args.steps,
+                                                        "downsample": stage[1] / args.steps,
+                                                        "ffa_snr": k_ms},
+                       "alg_bytes_per_step": bytes_job,
+                       "hbm_frac_whole_job": bytes_job / (ms * 1e-3) / 1e9 / peak,
+                       "parallelism": "trials sharded across GPUs" if world > 1 else "1 GPU"},
+            "roofline": roofline,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+            "plain_gpu": plain,
+            "batched_vs_plain": (value / world / plain["trials_per_s"]) if plain else None,
+        }
+        print(json.dumps(line), flush=True)
+    bs.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=3, choices=[1, 2, 3, 5])
+    ap.add_argument("--trials", type=int, default=None)
+    ap.add_argument("--cpu-sample", type=int, default=64)
+    ap.add_argument("--plain-trials", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.trials is None:
+        args.trials = {1: 1, 2: 1, 3: 512, 5: 1024}[args.config]
+    if args.impl == "reference":
+        return bench_reference(args)
+    return bench_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

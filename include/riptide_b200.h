@@ -1,0 +1,170 @@
+/*
+ * riptide_b200.h -- C ABI of the B200 (sm_100a) implementation of riptide's FFA search.
+ *
+ * Every function returns an int status (RT_OK on success); on failure rt_last_error()
+ * returns a message for the calling thread. RT_EINVAL corresponds to the reference raising
+ * std::invalid_argument (ValueError in Python) with the same message text.
+ *
+ * Pointers named d_* are CUDA device pointers; h_* are host pointers. `stream` is a
+ * cudaStream_t passed as void* (NULL = the legacy default stream). Kernels are enqueued
+ * asynchronously on `stream`; functions that need host results synchronise it themselves.
+ *
+ * Each entry point cites the reference interface it replaces (paths relative to the
+ * reference project: src/riptide/cpp/python_bindings.cpp is the pybind11 module
+ * `riptide.libcpp`).
+ */
+#ifndef RIPTIDE_B200_H
+#define RIPTIDE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RT_OK 0
+#define RT_EINVAL 1     /* invalid argument (ValueError)                   */
+#define RT_ECUDA 2      /* CUDA runtime error                              */
+#define RT_ENOMEM 3     /* device or host allocation failed                */
+#define RT_ETIMEOUT 4   /* a bounded wait inside a persistent kernel ran out */
+#define RT_EINTERNAL 5  /* a device-side plan check failed                 */
+
+/* Message of the last failing call on this thread. */
+const char* rt_last_error(void);
+/* Library version, 100 * major + minor. */
+int rt_version(void);
+
+/* ---------------------------------------------------------------------------------
+ * Drop-ins for the riptide.libcpp functions (device buffers).
+ * -------------------------------------------------------------------------------*/
+
+/* rollback: out = roll(x, -shift). Replaces python_bindings.cpp:44-52 (kernels.hpp:32-38). */
+int rt_rollback(const float* d_x, size_t size, size_t shift, float* d_out, void* stream);
+
+/* fused_rollback_add: out = x + roll(y, -shift). Replaces python_bindings.cpp:55-70
+ * (kernels.hpp:19-25). */
+int rt_fused_rollback_add(const float* d_x, const float* d_y, size_t size, size_t shift,
+                          float* d_out, void* stream);
+
+/* circular_prefix_sum over nsum elements, double accumulator. Replaces
+ * python_bindings.cpp:73-81 (kernels.hpp:73-101). d_out holds nsum floats. */
+int rt_circular_prefix_sum(const float* d_x, size_t size, size_t nsum, float* d_out,
+                           void* stream);
+
+/* ffa2: FFA transform of a rows x cols C-order block, bit-identical to the reference.
+ * Replaces python_bindings.cpp:84-96 (transforms.hpp:53-61). Allocates its own scratch for
+ * blocks larger than one CTA's shared memory. */
+int rt_ffa2(const float* d_in, size_t rows, size_t cols, float* d_out, void* stream);
+
+/* benchmark_ffa2: seconds per transform of a zero rows x cols block over `loops` runs
+ * (CUDA events). Replaces python_bindings.cpp:99-118. */
+int rt_benchmark_ffa2(size_t rows, size_t cols, size_t loops, double* h_seconds);
+
+/* snr2: boxcar S/N of `rows` profiles of `cols` bins for num_widths trial widths (host
+ * array). Output rows x num_widths. Replaces python_bindings.cpp:141-160 (snr.hpp:58-65);
+ * snr1 is the rows == 1 case (python_bindings.cpp:121-138). */
+int rt_snr2(const float* d_in, size_t rows, size_t cols, const uint64_t* h_widths,
+            size_t num_widths, float stdnoise, float* d_out, void* stream);
+
+/* downsample by a real factor 1 < f <= size; output floor(size / f) samples.
+ * Replaces python_bindings.cpp:163-177 (downsample.hpp:44-82). */
+int rt_downsample(const float* d_in, size_t size, double f, float* d_out, void* stream);
+
+/* floor(size / f) (downsample.hpp:21-24), host only. */
+size_t rt_downsampled_size(size_t size, double f);
+
+/* running_median of odd width < size with edge padding, exact. Replaces
+ * python_bindings.cpp:212-222 (running_median.hpp:100-132). */
+int rt_running_median(const float* d_in, size_t size, size_t width, float* d_out,
+                      void* stream);
+
+/* fast_running_median: approximate running median of a series (float64 output): mean-
+ * scrunch by int(max(1, width_samples / min_points)), exact running median of width
+ * min_points, linear interpolation back. Replaces running_medians.py:49-85. */
+int rt_fast_running_median(const float* d_in, size_t size, size_t width_samples,
+                           size_t min_points, double* d_out, void* stream);
+
+/* TimeSeries.deredden: out = float32(x - fast_running_median(x, round(width / tsamp),
+ * min_points)). Replaces time_series.py:95-124. */
+int rt_deredden(const float* d_in, size_t size, double tsamp, double width, size_t min_points,
+                float* d_out, void* stream);
+
+/* TimeSeries.normalise: out = float32((x - mean) / std), float64 statistics, population
+ * variance. Replaces time_series.py:67-93. */
+int rt_normalise(const float* d_in, size_t size, float* d_out, void* stream);
+
+/* Number of periodogram rows (periodogram.hpp:63-109), host only. */
+int rt_periodogram_length(size_t size, double tsamp, double period_min, double period_max,
+                          size_t bins_min, size_t bins_max, size_t* h_length);
+
+/* periodogram of one normalised series, through the batched engine (one trial).
+ * Replaces python_bindings.cpp:180-209 (periodogram.hpp:117-201). Outputs hold
+ * rt_periodogram_length() rows: periods (f64), foldbins (u32), snrs (rows x num_widths). */
+int rt_periodogram(const float* d_data, size_t size, double tsamp, const uint64_t* h_widths,
+                   size_t num_widths, double period_min, double period_max, size_t bins_min,
+                   size_t bins_max, double* d_periods, uint32_t* d_foldbins, float* d_snrs,
+                   void* stream);
+
+/* The same periodogram computed the plain way: one downsample launch per octave cycle and,
+ * per bins value, separate FFA, S/N and period launches with the FFA output in global
+ * memory -- the loop nest of periodogram.hpp:153-200 moved to the GPU as it stands. */
+int rt_periodogram_plain(const float* d_data, size_t size, double tsamp,
+                         const uint64_t* h_widths, size_t num_widths, double period_min,
+                         double period_max, size_t bins_min, size_t bins_max,
+                         double* d_periods, uint32_t* d_foldbins, float* d_snrs, void* stream);
+
+/* ---------------------------------------------------------------------------------
+ * Batched search: ffa_search (search.py:11-93) over many DM trials of uneven length.
+ * A plan holds everything that depends only on the lengths and the parameters.
+ * -------------------------------------------------------------------------------*/
+typedef struct rt_search_config {
+    double tsamp;          /* sampling time (s)                                   */
+    double period_min;     /* s                                                   */
+    double period_max;     /* s                                                   */
+    uint64_t bins_min;
+    uint64_t bins_max;
+    int deredden;          /* subtract the running median (time_series.py:95-124) */
+    double rmed_width;     /* running median width (s)                            */
+    uint64_t rmed_minpts;  /* odd                                                 */
+    int already_normalised;
+} rt_search_config;
+
+typedef struct rt_search_plan_stats_t {
+    uint64_t num_trials, num_cycles, num_transforms, num_work_items, num_multistage;
+    uint64_t total_rows;           /* periodogram rows of all trials              */
+    uint64_t total_samples;        /* input samples of all trials                 */
+    uint64_t downsampled_samples;  /* samples of all downsampled series           */
+    uint64_t folded_samples;       /* sum over transforms of rows * bins          */
+    uint64_t scrunch_factor;
+} rt_search_plan_stats_t;
+
+typedef struct rt_search_plan rt_search_plan;
+
+/* Builds the plan (host work only). widths: trial boxcar widths (all > 0, < bins_min). */
+int rt_search_plan_create(const uint64_t* h_lengths, size_t ntrials,
+                          const rt_search_config* cfg, const uint64_t* h_widths,
+                          size_t num_widths, rt_search_plan** plan);
+/* Row offsets of each trial in the packed outputs: ntrials + 1 entries. */
+int rt_search_plan_rows(const rt_search_plan* plan, uint64_t* h_row_offsets);
+int rt_search_plan_stats(const rt_search_plan* plan, rt_search_plan_stats_t* stats);
+/* Enqueues the search. d_data: the series packed back to back (plan order). Outputs are
+ * packed by trial (rt_search_plan_rows). d_normalised (optional, may be NULL) receives the
+ * dereddened + normalised series actually searched. Device buffers of the plan are
+ * allocated on the first run. Not reentrant per plan. */
+int rt_search_run(rt_search_plan* plan, const float* d_data, float* d_normalised,
+                  double* d_periods, uint32_t* d_foldbins, float* d_snrs, void* stream);
+/* Synchronises `stream` and reports a device-side failure of the last run. */
+int rt_search_check(rt_search_plan* plan, void* stream);
+/* Per-stage CUDA-event timing of rt_search_run (events recorded on the run's stream). */
+int rt_search_set_timing(rt_search_plan* plan, int enable);
+/* Milliseconds of the last timed run: h_ms[0] deredden + normalise statistics,
+ * h_ms[1] downsampling of all cycles, h_ms[2] the persistent FFA + S/N kernel; also the number
+ * of kernel launches the run made. Synchronises with the run. */
+int rt_search_last_timing(rt_search_plan* plan, float* h_ms, int* h_launches);
+void rt_search_plan_destroy(rt_search_plan* plan);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RIPTIDE_B200_H */

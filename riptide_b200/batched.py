@@ -1,0 +1,148 @@
+"""Batched FFA search: ffa_search over many DM trials of uneven length in one GPU pass.
+
+A ``BatchedSearch`` owns a plan (C ABI rt_search_plan_*): every (trial, octave cycle, bins)
+transform, its stage split and the work list of the persistent kernel. Plans depend only on
+the trial lengths and the search parameters, so one plan serves every batch of that shape.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib, libcpp
+from .ffautils import generate_width_trials
+from .periodogram import Periodogram
+
+
+class BatchedSearch(object):
+    """Search many series with the parameters of ffa_search (search.py:11-93)."""
+
+    def __init__(self, lengths, tsamp, period_min=1.0, period_max=30.0, bins_min=240,
+                 bins_max=260, ducy_max=0.20, wtsp=1.5, deredden=True, rmed_width=4.0,
+                 rmed_minpts=101, already_normalised=False, widths=None):
+        self.lengths = np.ascontiguousarray(np.asarray(lengths, dtype=np.uint64).ravel())
+        self.tsamp = float(tsamp)
+        self.widths = (np.asarray(widths) if widths is not None
+                       else generate_width_trials(bins_min, ducy_max=ducy_max, wtsp=wtsp))
+        cfg = _lib.SearchConfig(
+            tsamp=self.tsamp, period_min=float(period_min), period_max=float(period_max),
+            bins_min=int(bins_min), bins_max=int(bins_max), deredden=int(bool(deredden)),
+            rmed_width=float(rmed_width), rmed_minpts=int(rmed_minpts),
+            already_normalised=int(bool(already_normalised)))
+        self._cfg = cfg
+        w, wp = _lib.u64_array(self.widths)
+        lp = self.lengths.ctypes.data_as(_lib._u64p)
+        h = ctypes.c_void_p()
+        _lib.check(_lib.load().rt_search_plan_create(lp, self.lengths.size, ctypes.byref(cfg), wp,
+                                                     w.size, ctypes.byref(h)))
+        self._plan = h
+        rows = np.zeros(self.lengths.size + 1, dtype=np.uint64)
+        _lib.check(_lib.load().rt_search_plan_rows(h, rows.ctypes.data_as(_lib._u64p)))
+        self.row_offsets = rows.astype(np.int64)
+        st = _lib.PlanStats()
+        _lib.check(_lib.load().rt_search_plan_stats(h, ctypes.byref(st)))
+        self.stats = {k: int(getattr(st, k)) for k, _ in _lib.PlanStats._fields_}
+        self.sample_offsets = np.concatenate([[0], np.cumsum(self.lengths.astype(np.int64))])
+        self._out = None
+
+    # ------------------------------------------------------------------
+    @property
+    def num_trials(self):
+        return int(self.lengths.size)
+
+    @property
+    def total_rows(self):
+        return int(self.row_offsets[-1])
+
+    def allocate_outputs(self, device="cuda"):
+        """Device tensors (periods f64[L], foldbins i32[L], snrs f32[L, nw]) of the batch."""
+        torch = libcpp._t()
+        L, nw = self.total_rows, self.widths.size
+        return (torch.empty((L,), dtype=torch.float64, device=device),
+                torch.empty((L,), dtype=torch.int32, device=device),
+                torch.empty((L, nw), dtype=torch.float32, device=device))
+
+    def run(self, data, outputs=None, normalised=None, check=True):
+        """Search `data` (CUDA float32 tensor, all series packed back to back). Returns the
+        packed device outputs (periods, foldbins, snrs). Kernels run on the current torch
+        stream; `check` synchronises it and raises on a device-side failure."""
+        torch = libcpp._t()
+        if not (libcpp._is_cuda_tensor(data) and data.dtype == torch.float32 and data.is_contiguous()):
+            raise ValueError("data must be a contiguous float32 CUDA tensor")
+        if data.numel() != int(self.sample_offsets[-1]):
+            raise ValueError("data does not hold the planned number of samples")
+        if outputs is None:
+            if self._out is None:
+                self._out = self.allocate_outputs(data.device)
+            outputs = self._out
+        periods, foldbins, snrs = outputs
+        nptr = ctypes.c_void_p(normalised.data_ptr()) if normalised is not None else None
+        st = libcpp._stream()
+        _lib.check(_lib.load().rt_search_run(self._plan, ctypes.c_void_p(data.data_ptr()), nptr,
+                                             ctypes.c_void_p(periods.data_ptr()),
+                                             ctypes.c_void_p(foldbins.data_ptr()),
+                                             ctypes.c_void_p(snrs.data_ptr()), st))
+        if check:
+            _lib.check(_lib.load().rt_search_check(self._plan, st))
+        return outputs
+
+    def search(self, series, return_normalised=False):
+        """End-to-end search of host series (list of 1D arrays, or one packed array). Returns
+        a list of Periodogram (host numpy arrays), and the searched series if asked."""
+        torch = libcpp._t()
+        if isinstance(series, np.ndarray) and series.ndim == 1 and series.size == self.sample_offsets[-1]:
+            packed = np.ascontiguousarray(series, dtype=np.float32)
+        else:
+            packed = np.concatenate([np.asarray(s, dtype=np.float32).ravel() for s in series])
+        if packed.size != self.sample_offsets[-1]:
+            raise ValueError("series lengths do not match the plan")
+        host = torch.from_numpy(packed).pin_memory()
+        dev = host.to("cuda", non_blocking=True)
+        norm = torch.empty_like(dev) if return_normalised else None
+        periods, foldbins, snrs = self.run(dev, normalised=norm)
+        p = periods.cpu().numpy()
+        fb = foldbins.cpu().numpy().view(np.uint32)
+        s = snrs.cpu().numpy()
+        out = []
+        for i in range(self.num_trials):
+            a, b = self.row_offsets[i], self.row_offsets[i + 1]
+            md = {"tobs": float(self.lengths[i]) * self.tsamp}
+            out.append(Periodogram(self.widths, p[a:b], fb[a:b], s[a:b], metadata=md))
+        if return_normalised:
+            z = norm.cpu().numpy()
+            zs = [z[self.sample_offsets[i]:self.sample_offsets[i + 1]] for i in range(self.num_trials)]
+            return out, zs
+        return out
+
+    def enable_timing(self, enable=True):
+        """Record CUDA events around the stages of every run (see last_timing)."""
+        _lib.check(_lib.load().rt_search_set_timing(self._plan, int(bool(enable))))
+
+    def last_timing(self):
+        """(ms deredden+stats, ms downsample, ms FFA+S/N kernel, kernel launches) of the last
+        run with timing enabled."""
+        ms = (ctypes.c_float * 3)()
+        n = ctypes.c_int(0)
+        _lib.check(_lib.load().rt_search_last_timing(self._plan, ms, ctypes.byref(n)))
+        return float(ms[0]), float(ms[1]), float(ms[2]), int(n.value)
+
+    def close(self):
+        if getattr(self, "_plan", None):
+            _lib.load().rt_search_plan_destroy(self._plan)
+            self._plan = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ffa_search_batched(series, tsamp, **kwargs):
+    """ffa_search over a list of series sharing tsamp and search parameters. Returns a list
+    of Periodogram objects (host arrays)."""
+    lengths = [np.asarray(s).size for s in series]
+    bs = BatchedSearch(lengths, tsamp, **kwargs)
+    try:
+        return bs.search(series)
+    finally:
+        bs.close()

@@ -1,0 +1,1094 @@
+// Batched FFA search engine: many DM trials of uneven length searched in one pass.
+//
+// Stream of work for one run (all stream-ordered, capturable in a CUDA graph):
+//   1. deredden (time_series.py:95-124 / running_medians.py:40-85): mean-scrunch, exact
+//      running median of the scrunched series, linear interpolation back, subtraction;
+//   2. normalise (time_series.py:67-93): FP64 mean / variance per trial;
+//   3. one pass over every series producing the downsampled copy for every octave cycle
+//      (normalisation applied on the fly, cpp/periodogram.hpp:153-168);
+//   4. one persistent kernel that walks a precomputed list of FFA jobs (ffa_core.cuh) for all
+//      (trial, cycle, bins) transforms and writes the periodogram rows (S/N fused).
+// Transforms too large for one CTA are split in stages; jobs of a stage wait for the previous
+// stage through per-transform counters, and stage-0 jobs wait until their scratch slot is
+// released. Every wait is bounded and reports RT_ETIMEOUT instead of hanging.
+#include <string.h>
+
+#include <algorithm>
+#include <deque>
+#include <map>
+#include <vector>
+
+#include "common.cuh"
+#include "ffa_core.cuh"
+#include "kernels.cuh"
+#include "snr_core.cuh"
+
+namespace rt {
+
+struct XformRec {
+    unsigned long long src_off;  // row 0 of the folded series (offset in its arena)
+    unsigned long long out_row;  // first periodogram row of this transform
+    double tau;                  // sampling time of the folded series
+    int b, m, rows_eval;
+    float stdnoise;
+    int plan;                    // index into the stage-plan table
+    int seq;                     // multi-stage sequence number, -1 for single-stage transforms
+    int src_norm;                // 1: src is in the normalised series arena, 0: downsampled arena
+    int pad;
+};
+
+struct WorkItem {
+    int xform;
+    int stage_job;       // stage << 24 | job
+};
+
+// Shared-memory layout of the persistent kernel: job tree, S/N parameters, two level buffers.
+constexpr size_t kEngineTreeBytes = (sizeof(JobTree) + 255) & ~size_t(255);
+constexpr size_t kEngineSnrBytes = (sizeof(SnrParams) + 255) & ~size_t(255);
+constexpr size_t kEngineBufFloats =
+    (kFfaSmemBytes - kEngineTreeBytes - kEngineSnrBytes) / (2 * sizeof(float));
+RT_HD int engine_cap_rows(int b) { return (int)(kEngineBufFloats / ffa_stride(b)); }
+
+constexpr int kSlots = 16;           // scratch slots for multi-stage transforms
+constexpr int kPipelineLag = 2;      // stage s of transform i follows stage 0 of i + s*lag
+constexpr long long kSpinLimit = 20000000LL;  // bounded waits (about 2-20 s with backoff)
+
+struct EngineArgs {
+    const float* ds;         // downsampled series arena
+    const float* norm;       // normalised series arena (cycles with f == 1)
+    float* snrs;
+    double* periods;
+    uint32_t* foldbins;
+    const XformRec* xforms;
+    const WorkItem* items;
+    long long nitems;
+    const StagePlan* plans;
+    const int* widths;
+    int nw, nfast;
+    float* scratch;          // kSlots * 2 * slot_floats
+    size_t slot_floats;
+    int* done;               // [nseq * kMaxStages]
+    int* slot_release;       // [kSlots]
+    unsigned long long* ticket;
+    int* error;              // RT_OK or an error code
+};
+
+__device__ __forceinline__ int ld_acquire(const int* p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Bounded wait until *p >= target. Returns false (and records RT_ETIMEOUT) on timeout or if
+// another CTA already failed.
+__device__ bool wait_at_least(const int* p, int target, int* error)
+{
+    unsigned ns = 32;
+    for (long long it = 0; it < kSpinLimit; ++it) {
+        if (ld_acquire(p) >= target) return true;
+        if (ld_acquire(error) != RT_OK) return false;
+        __nanosleep(ns);
+        if (ns < 1024) ns <<= 1;
+    }
+    atomicExch(error, RT_ETIMEOUT);
+    return false;
+}
+
+template <int TPR>
+__device__ void final_stage_outputs(const JobTree& T, const XformRec& X, const EngineArgs& A,
+                                    SnrParams& S, float* buf0, float* buf1, int fstride,
+                                    int cap_rows)
+{
+    const Node r = T.nodes[0];
+    const int b = X.b;
+    const int cs = prefix_stride(b, S.wmax, TPR);
+    const int crows = (int)(((size_t)cap_rows * fstride) / cs);
+    float* snr_out = A.snrs + (size_t)X.out_row * S.nw;
+    for (int c0 = 0; c0 < r.hi - r.lo; c0 += crows) {
+        const int nr = min(crows, r.hi - r.lo - c0);
+        prefix_rows(buf0 + (size_t)c0 * fstride, fstride, nr, b, S.wmax, buf1, cs);
+        __syncthreads();
+        snr_rows_from_prefix<TPR, 17>(buf1, cs, nr, b, S, X.stdnoise,
+                                      snr_out + (size_t)(r.lo + c0) * S.nw, S.nw);
+        __syncthreads();
+    }
+    double* per_out = A.periods + X.out_row;
+    uint32_t* fb_out = A.foldbins + X.out_row;
+    for (int s = r.lo + threadIdx.x; s < r.hi; s += blockDim.x) {
+        per_out[s] = trial_period(X.tau, b, s, X.m);
+        fb_out[s] = (uint32_t)b;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, 1) k_search_persistent(EngineArgs A)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    JobTree& T = *reinterpret_cast<JobTree*>(smem);
+    SnrParams& S = *reinterpret_cast<SnrParams*>(smem + kEngineTreeBytes);
+    float* bufs = reinterpret_cast<float*>(smem + kEngineTreeBytes + kEngineSnrBytes);
+    __shared__ long long s_item;
+    __shared__ int s_ok;
+    __shared__ int s_b;
+    if (threadIdx.x == 0) s_b = -1;
+
+    for (;;) {
+        if (threadIdx.x == 0) {
+            s_item = (ld_acquire(A.error) != RT_OK) ? A.nitems
+                                                    : (long long)atomicAdd(A.ticket, 1ull);
+        }
+        __syncthreads();
+        const long long it = s_item;
+        if (it >= A.nitems) break;
+        const WorkItem W = A.items[it];
+        const XformRec X = A.xforms[W.xform];
+        const StagePlan& P = A.plans[X.plan];
+        const int stage = W.stage_job >> 24, job = W.stage_job & 0xffffff;
+        const bool last = stage == P.nstages - 1;
+        const JobSpec J = stage_job(X.m, X.rows_eval, P, stage, job);
+        const int b = X.b;
+        const int fstride = ffa_stride(b);
+        const int cap_rows = engine_cap_rows(b);
+        float* buf0 = bufs;
+        float* buf1 = bufs + (size_t)cap_rows * fstride;
+        float* slot = (X.seq >= 0) ? A.scratch + (size_t)(X.seq % kSlots) * 2 * A.slot_floats
+                                   : nullptr;
+        if (threadIdx.x == 0) {
+            s_ok = 1;
+            if (J.hi > J.lo && X.seq >= 0) {
+                bool ok;
+                if (stage == 0)
+                    ok = wait_at_least(A.slot_release + (X.seq % kSlots), X.seq / kSlots, A.error);
+                else
+                    ok = wait_at_least(A.done + (size_t)X.seq * kMaxStages + stage - 1,
+                                       P.jobs[stage - 1], A.error);
+                s_ok = ok ? 1 : 0;
+            }
+        }
+        if (b != s_b) {
+            // boxcar coefficients depend on b
+            __syncthreads();
+            snr_params_fill(S, A.widths, A.nw, A.nfast, b);
+            if (threadIdx.x == 0) s_b = b;
+        }
+        __syncthreads();
+        if (!s_ok) break;
+        if (J.hi > J.lo) {
+            const float* src =
+                (stage == 0) ? (X.src_norm ? A.norm : A.ds) + X.src_off
+                             : slot + (size_t)((stage - 1) & 1) * A.slot_floats;
+            build_job_tree(T, J, cap_rows);
+            if (T.error) {
+                if (threadIdx.x == 0) atomicExch(A.error, RT_EINTERNAL);
+                break;
+            }
+            run_job_levels(T, src, b, buf0, buf1, fstride);
+            if (last) {
+                if (snr_tpr(b) == 8)
+                    final_stage_outputs<8>(T, X, A, S, buf0, buf1, fstride, cap_rows);
+                else
+                    final_stage_outputs<16>(T, X, A, S, buf0, buf1, fstride, cap_rows);
+            } else {
+                store_root_rows(T, buf0, fstride, b, slot + (size_t)(stage & 1) * A.slot_floats);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && X.seq >= 0) {
+            __threadfence();
+            int* d = A.done + (size_t)X.seq * kMaxStages + stage;
+            const int prev = atomicAdd(d, 1);
+            if (last && prev + 1 == P.jobs[stage]) {
+                __threadfence();
+                atomicAdd(A.slot_release + (X.seq % kSlots), 1);
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Deredden / normalise (batched)
+// ------------------------------------------------------------------------------------
+struct TrialArrays {
+    const size_t* len;       // [T]
+    const size_t* off;       // [T] offsets into the packed series
+    const size_t* lo_len;    // [T] scrunched lengths
+    const size_t* lo_off;    // [T] offsets into the packed scrunched series
+};
+
+// lores[j] = float32 mean of x[j*k .. (j+1)*k) (running_medians.py:40-46). One warp per value.
+__global__ void k_scrunch(const float* __restrict__ x, TrialArrays A, int k,
+                          float* __restrict__ lores)
+{
+    const int trial = blockIdx.y;
+    const size_t nl = A.lo_len[trial];
+    const float* xr = x + A.off[trial];
+    float* o = lores + A.lo_off[trial];
+    const int lane = threadIdx.x & 31;
+    const size_t w0 = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
+    const size_t nwarp = ((size_t)gridDim.x * blockDim.x) >> 5;
+    for (size_t j = w0; j < nl; j += nwarp) {
+        double acc = 0.0;
+        for (int i = lane; i < k; i += 32) acc += (double)__ldg(xr + j * k + i);
+#pragma unroll
+        for (int o2 = 16; o2 > 0; o2 >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o2);
+        if (lane == 0) o[j] = __fdiv_rn(__double2float_rn(acc), (float)k);
+    }
+}
+
+constexpr int kStatThreads = 256;
+
+// y = float32(x - running median); per-block shifted sums for the statistics.
+// k > 1: rmed = np.interp(i, j*k + (k-1)/2, rmed_lores) in float64 (running_medians.py:82-85);
+// k == 1: rmed is the full-resolution float32 running median (float32 subtraction).
+__global__ void __launch_bounds__(kStatThreads)
+    k_dered(const float* __restrict__ x, TrialArrays A, int k, const float* __restrict__ rmed,
+            float* __restrict__ y, double* __restrict__ part, int blocks_per_trial)
+{
+    const int trial = blockIdx.y;
+    const size_t N = A.len[trial];
+    const float* xr = x + A.off[trial];
+    float* yr = y + A.off[trial];
+    const float* fp = rmed + (k > 1 ? A.lo_off[trial] : A.off[trial]);
+    const size_t nl = A.lo_len[trial];
+    const double half = 0.5 * (double)(k - 1);
+    double s1 = 0.0, s2 = 0.0;
+    const float shift = xr[0];
+    float shift_y;
+    {
+        // shift for the sums: y[0]
+        double r0;
+        if (k > 1) r0 = (double)fp[0];  // x = 0 <= xp[0]
+        else r0 = 0.0;
+        shift_y = (k > 1) ? __double2float_rn((double)shift - r0) : __fsub_rn(shift, fp[0]);
+    }
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N;
+         i += (size_t)blocks_per_trial * blockDim.x) {
+        const float xv = xr[i];
+        float yv;
+        if (k > 1) {
+            const double xi = (double)i;
+            double r;
+            const double x0 = half, xl = (double)(nl - 1) * k + half;
+            if (xi < x0) {
+                r = (double)fp[0];
+            } else if (xi >= xl) {
+                r = (double)fp[nl - 1];
+            } else {
+                long long j = (2LL * (long long)i - (k - 1)) / (2LL * k);
+                const double xj = (double)j * k + half;
+                if (xj == xi) {
+                    r = (double)fp[j];
+                } else {
+                    const double slope =
+                        __ddiv_rn(__dsub_rn((double)fp[j + 1], (double)fp[j]), (double)k);
+                    r = __dadd_rn(__dmul_rn(slope, __dsub_rn(xi, xj)), (double)fp[j]);
+                }
+            }
+            yv = __double2float_rn(__dsub_rn((double)xv, r));
+        } else {
+            yv = __fsub_rn(xv, fp[i]);
+        }
+        yr[i] = yv;
+        const double d = (double)yv - (double)shift_y;
+        s1 += d;
+        s2 += d * d;
+    }
+    // block reduction (fixed order)
+    __shared__ double r1[kStatThreads], r2[kStatThreads];
+    r1[threadIdx.x] = s1;
+    r2[threadIdx.x] = s2;
+    __syncthreads();
+    for (int o = kStatThreads / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            r1[threadIdx.x] += r1[threadIdx.x + o];
+            r2[threadIdx.x] += r2[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double* p = part + ((size_t)trial * blocks_per_trial + blockIdx.x) * 3;
+        p[0] = r1[0];
+        p[1] = r2[0];
+        p[2] = (double)shift_y;
+    }
+}
+
+// Same statistics without deredden (normalise only).
+__global__ void __launch_bounds__(kStatThreads)
+    k_sums(const float* __restrict__ x, TrialArrays A, double* __restrict__ part,
+           int blocks_per_trial)
+{
+    const int trial = blockIdx.y;
+    const size_t N = A.len[trial];
+    const float* xr = x + A.off[trial];
+    const float shift = xr[0];
+    double s1 = 0.0, s2 = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N;
+         i += (size_t)blocks_per_trial * blockDim.x) {
+        const double d = (double)xr[i] - (double)shift;
+        s1 += d;
+        s2 += d * d;
+    }
+    __shared__ double r1[kStatThreads], r2[kStatThreads];
+    r1[threadIdx.x] = s1;
+    r2[threadIdx.x] = s2;
+    __syncthreads();
+    for (int o = kStatThreads / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            r1[threadIdx.x] += r1[threadIdx.x + o];
+            r2[threadIdx.x] += r2[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double* p = part + ((size_t)trial * blocks_per_trial + blockIdx.x) * 3;
+        p[0] = r1[0];
+        p[1] = r2[0];
+        p[2] = (double)shift;
+    }
+}
+
+// mean and standard deviation per trial (population variance, ddof = 0).
+__global__ void k_stats(const double* __restrict__ part, const size_t* __restrict__ len,
+                        int blocks_per_trial, int ntrials, double* __restrict__ mean,
+                        double* __restrict__ norm)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntrials) return;
+    double s1 = 0.0, s2 = 0.0, shift = 0.0;
+    for (int b = 0; b < blocks_per_trial; ++b) {
+        const double* p = part + ((size_t)t * blocks_per_trial + b) * 3;
+        s1 += p[0];
+        s2 += p[1];
+        shift = p[2];
+    }
+    const double N = (double)len[t];
+    const double d = s1 / N;
+    const double var = s2 / N - d * d;
+    mean[t] = shift + d;
+    norm[t] = sqrt(var);
+}
+
+// fast_running_median output (running_medians.py:82-85): float64 interpolation of the
+// scrunched running median back to every sample.
+__global__ void k_interp_rmed(TrialArrays A, int k, const float* __restrict__ rmed,
+                              double* __restrict__ out)
+{
+    const int trial = blockIdx.y;
+    const size_t N = A.len[trial];
+    const float* fp = rmed + A.lo_off[trial];
+    const size_t nl = A.lo_len[trial];
+    double* o = out + A.off[trial];
+    const double half = 0.5 * (double)(k - 1);
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const double xi = (double)i;
+        const double xl = (double)(nl - 1) * k + half;
+        double r;
+        if (xi < half) {
+            r = (double)fp[0];
+        } else if (xi >= xl) {
+            r = (double)fp[nl - 1];
+        } else {
+            const long long j = (2LL * (long long)i - (k - 1)) / (2LL * k);
+            const double xj = (double)j * k + half;
+            if (xj == xi) {
+                r = (double)fp[j];
+            } else {
+                const double slope =
+                    __ddiv_rn(__dsub_rn((double)fp[j + 1], (double)fp[j]), (double)k);
+                r = __dadd_rn(__dmul_rn(slope, __dsub_rn(xi, xj)), (double)fp[j]);
+            }
+        }
+        o[i] = r;
+    }
+}
+
+// z = float32((x - mean) / norm) in float64 (time_series.py:91-93).
+__global__ void k_normalise(const float* __restrict__ x, TrialArrays A, const double* mean,
+                            const double* norm, float* __restrict__ z)
+{
+    const int trial = blockIdx.y;
+    const size_t N = A.len[trial];
+    const float* xr = x + A.off[trial];
+    float* zr = z + A.off[trial];
+    const double m = mean[trial], s = norm[trial];
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N;
+         i += (size_t)gridDim.x * blockDim.x)
+        zr[i] = __double2float_rn(__ddiv_rn(__dsub_rn((double)xr[i], m), s));
+}
+
+// ------------------------------------------------------------------------------------
+// Plan
+// ------------------------------------------------------------------------------------
+struct SearchPlan {
+    // configuration
+    rt_search_config cfg;
+    std::vector<int> widths;
+    int nfast = 0;
+    std::vector<size_t> lengths, offsets;
+    size_t total_len = 0, max_len = 0;
+    // cycles (cpp/periodogram.hpp:135-158)
+    std::vector<double> f, tau, pms;
+    std::vector<int> use_seg, skip;
+    // per trial
+    std::vector<size_t> out_rows_off;   // [T+1]
+    std::vector<size_t> ds_off;         // [T * C] offsets into the downsample arena
+    size_t ds_total = 0;
+    bool has_unit_factor = false;       // a cycle folds the series itself (f == 1)
+    // deredden
+    int scrunch = 1, rmed_width = 0;
+    std::vector<size_t> lo_len, lo_off;
+    size_t lo_total = 0, max_lo = 0;
+    // work
+    std::vector<StagePlan> plans;
+    std::vector<XformRec> xforms;
+    std::vector<WorkItem> items;
+    int nseq = 0;
+    size_t slot_floats = 0;
+    // device buffers
+    bool dev_ready = false;
+    int* d_widths = nullptr;
+    XformRec* d_xforms = nullptr;
+    WorkItem* d_items = nullptr;
+    StagePlan* d_plans = nullptr;
+    float* d_scratch = nullptr;
+    int* d_counters = nullptr;          // done + slot_release + error
+    unsigned long long* d_ticket = nullptr;
+    float* d_ds = nullptr;
+    float* d_y = nullptr;               // dereddened series
+    float* d_norm = nullptr;            // normalised copy (when a cycle has f == 1)
+    float* d_lores = nullptr;
+    float* d_rmed = nullptr;
+    double* d_part = nullptr;
+    double* d_mean = nullptr;
+    double* d_normv = nullptr;
+    size_t* d_len = nullptr;
+    size_t* d_off = nullptr;
+    size_t* d_lo_len = nullptr;
+    size_t* d_lo_off = nullptr;
+    double* d_f = nullptr;
+    int* d_useseg = nullptr;
+    size_t* d_dsoff = nullptr;
+    int stat_blocks = 64;
+    // optional per-stage CUDA-event timing: deredden+normalise, downsample, FFA + S/N
+    bool timing = false;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    int launches_last_run = 0;
+};
+
+static int plan_cycles(SearchPlan& P)
+{
+    const rt_search_config& c = P.cfg;
+    // periodogram.hpp:25-40, same messages and order
+    if (!(c.tsamp > 0)) return set_error(RT_EINVAL, "tsamp must be > 0");
+    if (!(c.period_min > 0)) return set_error(RT_EINVAL, "period_min must be > 0");
+    if (!(c.period_max > c.period_min)) return set_error(RT_EINVAL, "period_max must be > period_min");
+    if (!(c.bins_min > 1)) return set_error(RT_EINVAL, "bins_min must be > 1");
+    if (!(c.bins_max >= c.bins_min)) return set_error(RT_EINVAL, "bins_max must be >= bins_min");
+    if (!(c.period_min >= c.tsamp * c.bins_min))
+        return set_error(RT_EINVAL, "Must have: period_min >= tsamp * bins_min ");
+    if (c.bins_max > 4096) return set_error(RT_EINVAL, "bins_max above 4096 is not supported");
+    const double ds_ini = c.period_min / (c.tsamp * c.bins_min);
+    const double ds_geo = (c.bins_max + 1.0) / c.bins_min;
+    const size_t nds = (size_t)ceil(log(c.period_max / c.period_min) / log(ds_geo));
+    if (nds > (size_t)kDsMaxCycles)
+        return set_error(RT_EINVAL, "too many downsampling cycles (%zu)", nds);
+    for (size_t i = 0; i < nds; ++i) {
+        const double f = ds_ini * pow(ds_geo, (double)i);
+        P.f.push_back(f);
+        P.tau.push_back(f * c.tsamp);
+        P.pms.push_back(c.period_max / (f * c.tsamp));
+        P.skip.push_back(f == 1 ? 1 : 0);
+        P.use_seg.push_back((f != 1 && ds_use_segments(f)) ? 1 : 0);
+        if (f == 1) P.has_unit_factor = true;
+    }
+    return RT_OK;
+}
+
+// Emits the work items of all transforms. Order: (trial, cycle, bins); for a transform that
+// needs several stages, stage s is emitted after the stage-0 jobs of kPipelineLag * s further
+// multi-stage transforms, so that its wait usually finds the previous stage complete.
+static int plan_build(SearchPlan& P)
+{
+    RT_TRY(plan_cycles(P));
+    const rt_search_config& c = P.cfg;
+    const int T = (int)P.lengths.size();
+    const int C = (int)P.f.size();
+    P.out_rows_off.assign(T + 1, 0);
+    P.ds_off.assign((size_t)T * C, 0);
+    std::map<std::pair<int, long long>, int> plan_index;
+    struct Deferred {
+        int xform, stage, due;
+    };
+    std::deque<Deferred> deferred;
+    int stage0_count = 0;
+
+    auto emit_stage = [&](int xi, int stage) {
+        const StagePlan& sp = P.plans[P.xforms[xi].plan];
+        for (int j = 0; j < sp.jobs[stage]; ++j) P.items.push_back({xi, (stage << 24) | j});
+    };
+
+    size_t ds_total = 0;
+    for (int t = 0; t < T; ++t) {
+        const size_t N = P.lengths[t];
+        size_t rows_total = 0;
+        for (int ci = 0; ci < C; ++ci) {
+            const double f = P.f[ci];
+            const size_t n = downsampled_size(N, f);
+            if (f != 1) {
+                // downsample.hpp:11-16 (the reference downsamples every cycle)
+                if (!((f > 1.0) && (f <= (double)N)))
+                    return set_error(RT_EINVAL, "Downsampling factor must verify: 1 < f <= size");
+                P.ds_off[(size_t)t * C + ci] = ds_total;
+                ds_total += n;
+            }
+            const size_t bstop = std::min({(size_t)c.bins_max, n, (size_t)P.pms[ci]});
+            for (size_t b = c.bins_min; b <= bstop; ++b) {
+                const size_t rows = n / b;
+                const size_t re = rows_to_evaluate(rows, b, P.pms[ci]);
+                if (re == 0) continue;
+                if (rows >= (1u << 24))
+                    return set_error(RT_EINVAL, "transform of %zu rows is too large", rows);
+                const int capr = engine_cap_rows((int)b);
+                const auto key = std::make_pair((int)rows, (long long)re * 8192 + (long long)b);
+                int pi;
+                auto itp = plan_index.find(key);
+                if (itp == plan_index.end()) {
+                    StagePlan sp;
+                    if (capr < 4 || !plan_stages((int)rows, (int)re, capr, &sp))
+                        return set_error(RT_EINVAL, "no device plan for a %zu x %zu transform", rows, b);
+                    pi = (int)P.plans.size();
+                    P.plans.push_back(sp);
+                    plan_index[key] = pi;
+                } else {
+                    pi = itp->second;
+                }
+                XformRec X;
+                memset(&X, 0, sizeof(X));
+                X.src_off = (f != 1) ? P.ds_off[(size_t)t * C + ci] : P.offsets[t];
+                X.src_norm = (f != 1) ? 0 : 1;
+                X.out_row = P.out_rows_off[t] + rows_total;
+                X.tau = P.tau[ci];
+                X.b = (int)b;
+                X.m = (int)rows;
+                X.rows_eval = (int)re;
+                X.stdnoise = (float)sqrt((double)rows * downsampled_variance(N, f));
+                X.plan = pi;
+                X.seq = -1;
+                const int xi = (int)P.xforms.size();
+                const StagePlan& sp = P.plans[pi];
+                if (sp.nstages > 1) {
+                    X.seq = P.nseq++;
+                    P.slot_floats = std::max(P.slot_floats, rows * b);
+                }
+                P.xforms.push_back(X);
+                rows_total += re;
+                emit_stage(xi, 0);
+                if (sp.nstages > 1) {
+                    ++stage0_count;
+                    for (int s = 1; s < sp.nstages; ++s)
+                        deferred.push_back({xi, s, stage0_count + s * kPipelineLag});
+                    std::stable_sort(deferred.begin(), deferred.end(),
+                                     [](const Deferred& a, const Deferred& b2) { return a.due < b2.due; });
+                    while (!deferred.empty() && deferred.front().due <= stage0_count) {
+                        emit_stage(deferred.front().xform, deferred.front().stage);
+                        deferred.pop_front();
+                    }
+                }
+            }
+        }
+        P.out_rows_off[t + 1] = P.out_rows_off[t] + rows_total;
+    }
+    while (!deferred.empty()) {
+        emit_stage(deferred.front().xform, deferred.front().stage);
+        deferred.pop_front();
+    }
+    P.ds_total = ds_total;
+    // The slot of sequence q is reused by q + kSlots; all items of q precede the stage-0 items
+    // of q + kSlots in the work order because kSlots > (kMaxStages - 1) * kPipelineLag + 1.
+    static_assert(kSlots > (kMaxStages - 1) * kPipelineLag + 1, "slot ring too small");
+
+    // deredden geometry (time_series.py:119, running_medians.py:72-80)
+    P.lo_len.assign(T, 0);
+    P.lo_off.assign(T, 0);
+    if (c.deredden) {
+        const double ws = nearbyint(c.rmed_width / c.tsamp);  // Python round(): half to even
+        if (!(ws >= 1)) return set_error(RT_EINVAL, "rmed_width is shorter than one sample");
+        P.rmed_width = (int)ws;
+        if (!(c.rmed_minpts % 2)) return set_error(RT_EINVAL, "min_points must be an odd number");
+        const double sf = std::max(1.0, ws / (double)c.rmed_minpts);
+        P.scrunch = (int)sf;
+        const int w = P.scrunch == 1 ? P.rmed_width : (int)c.rmed_minpts;
+        if (!(w % 2)) return set_error(RT_EINVAL, "width must be an odd number");
+        size_t lo_total = 0;
+        for (int t = 0; t < T; ++t) {
+            const size_t nl = P.scrunch == 1 ? P.lengths[t] : P.lengths[t] / P.scrunch;
+            if (!((size_t)w < nl)) return set_error(RT_EINVAL, "width must be < size");
+            P.lo_len[t] = nl;
+            P.lo_off[t] = lo_total;
+            lo_total += nl;
+            P.max_lo = std::max(P.max_lo, nl);
+        }
+        P.lo_total = lo_total;
+    }
+    return RT_OK;
+}
+
+static void plan_free_device(SearchPlan& P)
+{
+    void* ptrs[] = {P.d_widths, P.d_xforms, P.d_items, P.d_plans, P.d_scratch, P.d_counters,
+                    P.d_ticket, P.d_ds, P.d_y, P.d_norm, P.d_lores, P.d_rmed, P.d_part,
+                    P.d_mean, P.d_normv, P.d_len, P.d_off, P.d_lo_len, P.d_lo_off, P.d_f,
+                    P.d_useseg, P.d_dsoff};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    P.dev_ready = false;
+}
+
+template <class T>
+static int dalloc(T** p, size_t n)
+{
+    if (n == 0) n = 1;
+    RT_TRY_CUDA(cudaMalloc((void**)p, n * sizeof(T)));
+    return RT_OK;
+}
+
+template <class T>
+static int upload(T** p, const std::vector<T>& v)
+{
+    RT_TRY(dalloc(p, v.size()));
+    if (!v.empty())
+        RT_TRY_CUDA(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return RT_OK;
+}
+
+static int plan_prepare_device(SearchPlan& P)
+{
+    if (P.dev_ready) return RT_OK;
+    const int T = (int)P.lengths.size();
+    RT_TRY(upload(&P.d_widths, P.widths));
+    RT_TRY(upload(&P.d_items, P.items));
+    RT_TRY(upload(&P.d_plans, P.plans));
+    RT_TRY(upload(&P.d_xforms, P.xforms));
+    RT_TRY(dalloc(&P.d_scratch, (size_t)kSlots * 2 * std::max<size_t>(P.slot_floats, 1)));
+    RT_TRY(dalloc(&P.d_counters, (size_t)P.nseq * kMaxStages + kSlots + 1));
+    RT_TRY(dalloc(&P.d_ticket, 1));
+    RT_TRY(dalloc(&P.d_ds, P.ds_total));
+    if (P.cfg.deredden) {
+        RT_TRY(dalloc(&P.d_y, P.total_len));
+        RT_TRY(dalloc(&P.d_rmed, P.scrunch > 1 ? P.lo_total : P.total_len));
+        if (P.scrunch > 1) RT_TRY(dalloc(&P.d_lores, P.lo_total));
+    }
+    if (P.has_unit_factor) RT_TRY(dalloc(&P.d_norm, P.total_len));
+    RT_TRY(dalloc(&P.d_part, (size_t)T * P.stat_blocks * 3));
+    RT_TRY(dalloc(&P.d_mean, T));
+    RT_TRY(dalloc(&P.d_normv, T));
+    RT_TRY(upload(&P.d_len, P.lengths));
+    RT_TRY(upload(&P.d_off, P.offsets));
+    RT_TRY(upload(&P.d_lo_len, P.lo_len));
+    RT_TRY(upload(&P.d_lo_off, P.lo_off));
+    RT_TRY(upload(&P.d_f, P.f));
+    RT_TRY(upload(&P.d_useseg, P.use_seg));
+    RT_TRY(upload(&P.d_dsoff, P.ds_off));
+    P.dev_ready = true;
+    return RT_OK;
+}
+
+static int engine_grid()
+{
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_search_persistent, kThreads,
+                                                  kFfaSmemBytes);
+    return std::max(1, sms * std::max(per, 1));
+}
+
+// Launches the whole search of the plan on `st`. data: packed input series (device).
+static int plan_run(SearchPlan& P, const float* data, float* normalised_out, double* periods,
+                    uint32_t* foldbins, float* snrs, cudaStream_t st)
+{
+    RT_TRY(plan_prepare_device(P));
+    const int T = (int)P.lengths.size();
+    const int C = (int)P.f.size();
+    TrialArrays TA{P.d_len, P.d_off, P.d_lo_len, P.d_lo_off};
+    const float* series = data;  // series before normalisation
+    int launches = 0;
+    if (P.timing) RT_TRY_CUDA(cudaEventRecord(P.ev[0], st));
+    if (P.cfg.deredden) {
+        const int k = P.scrunch;
+        if (k > 1) {
+            dim3 g((unsigned)std::min<size_t>((P.max_lo * 32 + 255) / 256, 4096), (unsigned)T);
+            k_scrunch<<<g, 256, 0, st>>>(data, TA, k, P.d_lores);
+            RT_TRY_CUDA(cudaGetLastError());
+            RT_TRY(launch_running_median(P.d_lores, P.d_lo_len, P.d_lo_off, T, P.max_lo,
+                                         (int)P.cfg.rmed_minpts, P.d_rmed, st));
+            launches += 2;
+        } else {
+            RT_TRY(launch_running_median(data, P.d_len, P.d_off, T, P.max_len, P.rmed_width,
+                                         P.d_rmed, st));
+            launches += 1;
+        }
+        dim3 g((unsigned)P.stat_blocks, (unsigned)T);
+        k_dered<<<g, kStatThreads, 0, st>>>(data, TA, k, P.d_rmed, P.d_y, P.d_part,
+                                            P.stat_blocks);
+        RT_TRY_CUDA(cudaGetLastError());
+        launches += 1;
+        series = P.d_y;
+    } else if (!P.cfg.already_normalised) {
+        dim3 g((unsigned)P.stat_blocks, (unsigned)T);
+        k_sums<<<g, kStatThreads, 0, st>>>(data, TA, P.d_part, P.stat_blocks);
+        RT_TRY_CUDA(cudaGetLastError());
+        launches += 1;
+    }
+    const bool affine = !P.cfg.already_normalised;
+    if (affine) {
+        k_stats<<<(T + 127) / 128, 128, 0, st>>>(P.d_part, P.d_len, P.stat_blocks, T, P.d_mean,
+                                                 P.d_normv);
+        RT_TRY_CUDA(cudaGetLastError());
+        launches += 1;
+    }
+    if (P.timing) RT_TRY_CUDA(cudaEventRecord(P.ev[1], st));
+    // The normalised series is materialised by the downsampler when the caller wants it or
+    // when a cycle folds it directly (f == 1); without normalisation it is `series` itself.
+    float* zdst = normalised_out ? normalised_out : (P.has_unit_factor && affine ? P.d_norm : nullptr);
+    const float* zsrc = affine ? (zdst ? zdst : series) : series;
+    if (!affine && normalised_out && normalised_out != series)
+        RT_TRY_CUDA(cudaMemcpyAsync(normalised_out, series, P.total_len * sizeof(float),
+                                    cudaMemcpyDeviceToDevice, st));
+    DsJob job;
+    job.in = series;
+    job.in_off = P.d_off;
+    job.lengths = P.d_len;
+    job.mean = affine ? P.d_mean : nullptr;
+    job.norm = affine ? P.d_normv : nullptr;
+    job.norm_out = affine ? zdst : nullptr;
+    job.f = P.d_f;
+    job.use_seg = P.d_useseg;
+    job.out = P.d_ds;
+    job.out_off = P.d_dsoff;
+    job.ncycles = C;
+    job.use_seg_host = P.use_seg.data();
+    job.skip_host = P.skip.data();
+    RT_TRY(launch_downsample(job, T, P.max_len, st));
+    {
+        bool seg = job.norm_out != nullptr;
+        for (int c = 0; c < C; ++c) {
+            seg |= P.use_seg[c] != 0;
+            launches += (!P.use_seg[c] && !P.skip[c]) ? 1 : 0;
+        }
+        launches += seg ? 1 : 0;
+    }
+    if (P.timing) RT_TRY_CUDA(cudaEventRecord(P.ev[2], st));
+    // counters
+    const size_t ncounters = (size_t)P.nseq * kMaxStages + kSlots + 1;
+    RT_TRY_CUDA(cudaMemsetAsync(P.d_counters, 0, ncounters * sizeof(int), st));
+    RT_TRY_CUDA(cudaMemsetAsync(P.d_ticket, 0, sizeof(unsigned long long), st));
+    EngineArgs A;
+    A.ds = P.d_ds;
+    A.norm = zsrc;
+    A.snrs = snrs;
+    A.periods = periods;
+    A.foldbins = foldbins;
+    A.xforms = P.d_xforms;
+    A.items = P.d_items;
+    A.nitems = (long long)P.items.size();
+    A.plans = P.d_plans;
+    A.widths = P.d_widths;
+    A.nw = (int)P.widths.size();
+    A.nfast = P.nfast;
+    A.scratch = P.d_scratch;
+    A.slot_floats = P.slot_floats;
+    A.done = P.d_counters;
+    A.slot_release = P.d_counters + (size_t)P.nseq * kMaxStages;
+    A.error = A.slot_release + kSlots;
+    A.ticket = P.d_ticket;
+    RT_TRY_CUDA(cudaFuncSetAttribute(k_search_persistent,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kFfaSmemBytes));
+    if (A.nitems > 0) {
+        k_search_persistent<<<engine_grid(), kThreads, kFfaSmemBytes, st>>>(A);
+        RT_TRY_CUDA(cudaGetLastError());
+        launches += 1;
+    }
+    if (P.timing) RT_TRY_CUDA(cudaEventRecord(P.ev[3], st));
+    P.launches_last_run = launches;
+    return RT_OK;
+}
+
+static int plan_check_error(SearchPlan& P, cudaStream_t st)
+{
+    int err = 0;
+    RT_TRY_CUDA(cudaMemcpyAsync(&err, P.d_counters + (size_t)P.nseq * kMaxStages + kSlots,
+                                sizeof(int), cudaMemcpyDeviceToHost, st));
+    RT_TRY_CUDA(cudaStreamSynchronize(st));
+    if (err == RT_ETIMEOUT)
+        return set_error(RT_ETIMEOUT, "a bounded wait in the search kernel ran out");
+    if (err != RT_OK) return set_error(err, "the search kernel reported error %d", err);
+    return RT_OK;
+}
+
+}  // namespace rt
+
+// ====================================================================================
+// C ABI
+// ====================================================================================
+using namespace rt;
+
+struct rt_search_plan {
+    SearchPlan p;
+};
+
+extern "C" int rt_search_plan_create(const uint64_t* lengths, size_t ntrials,
+                                     const rt_search_config* cfg, const uint64_t* widths,
+                                     size_t num_widths, rt_search_plan** out)
+{
+    if (!out || !cfg || (!lengths && ntrials) || (!widths && num_widths))
+        return set_error(RT_EINVAL, "null argument");
+    *out = nullptr;
+    if (ntrials == 0) return set_error(RT_EINVAL, "at least one time series is required");
+    if (num_widths == 0 || num_widths > (size_t)kMaxWidths)
+        return set_error(RT_EINVAL, "between 1 and %d trial widths are supported", kMaxWidths);
+    rt_search_plan* h = new (std::nothrow) rt_search_plan();
+    if (!h) return set_error(RT_ENOMEM, "out of host memory");
+    SearchPlan& P = h->p;
+    P.cfg = *cfg;
+    for (size_t i = 0; i < num_widths; ++i) {
+        // snr.hpp:21-31
+        if (!(widths[i] > 0 && widths[i] < cfg->bins_min)) {
+            delete h;
+            return set_error(RT_EINVAL, "trial widths must be all > 0 and < columns");
+        }
+        P.widths.push_back((int)widths[i]);
+    }
+    P.nfast = detect_fast_widths(P.widths.data(), (int)P.widths.size());
+    if (P.nfast && P.widths.size() > 10 && cfg->bins_min <= 42) P.nfast = 0;
+    for (size_t t = 0; t < ntrials; ++t) {
+        if (lengths[t] == 0 || lengths[t] >= (1ull << 40)) {
+            delete h;
+            return set_error(RT_EINVAL, "time series %zu has an unsupported length", t);
+        }
+        P.lengths.push_back((size_t)lengths[t]);
+        P.offsets.push_back(P.total_len);
+        P.total_len += lengths[t];
+        P.max_len = std::max(P.max_len, (size_t)lengths[t]);
+    }
+    int s = plan_build(P);
+    if (s != RT_OK) {
+        delete h;
+        return s;
+    }
+    *out = h;
+    return RT_OK;
+}
+
+extern "C" int rt_search_plan_rows(const rt_search_plan* plan, uint64_t* row_offsets)
+{
+    if (!plan || !row_offsets) return set_error(RT_EINVAL, "null argument");
+    for (size_t i = 0; i < plan->p.out_rows_off.size(); ++i) row_offsets[i] = plan->p.out_rows_off[i];
+    return RT_OK;
+}
+
+extern "C" int rt_search_plan_stats(const rt_search_plan* plan, rt_search_plan_stats_t* st)
+{
+    if (!plan || !st) return set_error(RT_EINVAL, "null argument");
+    const SearchPlan& P = plan->p;
+    memset(st, 0, sizeof(*st));
+    st->num_trials = P.lengths.size();
+    st->num_cycles = P.f.size();
+    st->num_transforms = P.xforms.size();
+    st->num_work_items = P.items.size();
+    st->num_multistage = (uint64_t)P.nseq;
+    st->total_rows = P.out_rows_off.back();
+    st->total_samples = P.total_len;
+    st->downsampled_samples = P.ds_total;
+    uint64_t fold = 0;
+    for (const XformRec& X : P.xforms) fold += (uint64_t)X.m * X.b;
+    st->folded_samples = fold;
+    st->scrunch_factor = (uint64_t)P.scrunch;
+    return RT_OK;
+}
+
+extern "C" int rt_search_run(rt_search_plan* plan, const float* data, float* normalised_out,
+                             double* periods, uint32_t* foldbins, float* snrs, void* stream)
+{
+    if (!plan || !data || !periods || !foldbins || !snrs) return set_error(RT_EINVAL, "null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    return plan_run(plan->p, data, normalised_out, periods, foldbins, snrs, st);
+}
+
+extern "C" int rt_search_check(rt_search_plan* plan, void* stream)
+{
+    if (!plan) return set_error(RT_EINVAL, "null argument");
+    if (!plan->p.dev_ready) return RT_OK;
+    return plan_check_error(plan->p, (cudaStream_t)stream);
+}
+
+extern "C" int rt_search_set_timing(rt_search_plan* plan, int enable)
+{
+    if (!plan) return set_error(RT_EINVAL, "null argument");
+    SearchPlan& P = plan->p;
+    if (enable && !P.ev[0])
+        for (int i = 0; i < 4; ++i) RT_TRY_CUDA(cudaEventCreate(&P.ev[i]));
+    P.timing = enable != 0;
+    return RT_OK;
+}
+
+extern "C" int rt_search_last_timing(rt_search_plan* plan, float* h_ms, int* h_launches)
+{
+    if (!plan || !h_ms) return set_error(RT_EINVAL, "null argument");
+    SearchPlan& P = plan->p;
+    if (!P.timing || !P.ev[0]) return set_error(RT_EINVAL, "timing is not enabled on this plan");
+    RT_TRY_CUDA(cudaEventSynchronize(P.ev[3]));
+    for (int i = 0; i < 3; ++i) RT_TRY_CUDA(cudaEventElapsedTime(&h_ms[i], P.ev[i], P.ev[i + 1]));
+    if (h_launches) *h_launches = P.launches_last_run;
+    return RT_OK;
+}
+
+extern "C" void rt_search_plan_destroy(rt_search_plan* plan)
+{
+    if (!plan) return;
+    cudaDeviceSynchronize();
+    for (int i = 0; i < 4; ++i)
+        if (plan->p.ev[i]) cudaEventDestroy(plan->p.ev[i]);
+    plan_free_device(plan->p);
+    delete plan;
+}
+
+// ------------------------------------------------------------------------------------
+// Single-series deredden / normalise (TimeSeries.deredden / normalise, fast_running_median)
+// ------------------------------------------------------------------------------------
+namespace {
+struct OneSeries {
+    size_t v[4];  // len, off, lo_len, lo_off
+};
+}  // namespace
+
+static int one_series_arrays(size_t N, size_t nl, size_t** d, cudaStream_t st, TrialArrays* A)
+{
+    OneSeries h{{N, 0, nl, 0}};
+    RT_TRY_CUDA(cudaMallocAsync((void**)d, sizeof(h), st));
+    RT_TRY_CUDA(cudaMemcpyAsync(*d, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+    A->len = *d;
+    A->off = *d + 1;
+    A->lo_len = *d + 2;
+    A->lo_off = *d + 3;
+    return RT_OK;
+}
+
+// width_samples / min_points -> (scrunch factor, running-median width, scrunched length)
+static int rmed_geometry(size_t N, size_t width_samples, size_t minpts, int* k, int* w, size_t* nl)
+{
+    // running_medians.py:72-80
+    if (!(minpts % 2)) return set_error(RT_EINVAL, "min_points must be an odd number");
+    *k = (int)std::max(1.0, (double)width_samples / (double)minpts);
+    *w = (*k == 1) ? (int)width_samples : (int)minpts;
+    *nl = (*k == 1) ? N : N / (size_t)*k;
+    // running_median.hpp:103-107
+    if (!(*w % 2)) return set_error(RT_EINVAL, "width must be an odd number");
+    if (!((size_t)*w < *nl)) return set_error(RT_EINVAL, "width must be < size");
+    return RT_OK;
+}
+
+extern "C" int rt_fast_running_median(const float* d_x, size_t size, size_t width_samples,
+                                      size_t min_points, double* d_out, void* stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    int k, w;
+    size_t nl;
+    RT_TRY(rmed_geometry(size, width_samples, min_points, &k, &w, &nl));
+    size_t* d = nullptr;
+    TrialArrays A;
+    RT_TRY(one_series_arrays(size, nl, &d, st, &A));
+    float *lores = nullptr, *rmed = nullptr;
+    int s = RT_OK;
+    if (k > 1) {
+        RT_TRY_CUDA(cudaMallocAsync((void**)&lores, nl * sizeof(float), st));
+        RT_TRY_CUDA(cudaMallocAsync((void**)&rmed, nl * sizeof(float), st));
+        k_scrunch<<<dim3((unsigned)std::min<size_t>((nl * 32 + 255) / 256, 4096), 1), 256, 0, st>>>(
+            d_x, A, k, lores);
+        s = launch_running_median(lores, A.lo_len, A.lo_off, 1, nl, w, rmed, st);
+        if (s == RT_OK) {
+            k_interp_rmed<<<dim3(std::max(1, (int)std::min<size_t>((size + 255) / 256, 4096)), 1), 256, 0, st>>>(
+                A, k, rmed, d_out);
+            s = check_cuda(cudaGetLastError(), "fast_running_median");
+        }
+    } else {
+        // no scrunching: the exact running median (float32), widened to float64
+        RT_TRY_CUDA(cudaMallocAsync((void**)&rmed, size * sizeof(float), st));
+        s = launch_running_median(d_x, A.len, A.off, 1, size, w, rmed, st);
+        if (s == RT_OK) {
+            k_interp_rmed<<<dim3(std::max(1, (int)std::min<size_t>((size + 255) / 256, 4096)), 1), 256, 0, st>>>(
+                TrialArrays{A.len, A.off, A.len, A.off}, 1, rmed, d_out);
+            s = check_cuda(cudaGetLastError(), "fast_running_median");
+        }
+    }
+    if (lores) cudaFreeAsync(lores, st);
+    if (rmed) cudaFreeAsync(rmed, st);
+    cudaFreeAsync(d, st);
+    if (s == RT_OK) s = check_cuda(cudaStreamSynchronize(st), "fast_running_median");
+    return s;
+}
+
+extern "C" int rt_deredden(const float* d_x, size_t size, double tsamp, double width,
+                           size_t min_points, float* d_out, void* stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    const double ws = nearbyint(width / tsamp);  // int(round(width / tsamp)), half to even
+    if (!(ws >= 1)) return set_error(RT_EINVAL, "width is shorter than one sample");
+    int k, w;
+    size_t nl;
+    RT_TRY(rmed_geometry(size, (size_t)ws, min_points, &k, &w, &nl));
+    size_t* d = nullptr;
+    TrialArrays A;
+    RT_TRY(one_series_arrays(size, nl, &d, st, &A));
+    float *lores = nullptr, *rmed = nullptr;
+    double* part = nullptr;
+    int s = RT_OK;
+    const int blocks = 64;
+    RT_TRY_CUDA(cudaMallocAsync((void**)&part, blocks * 3 * sizeof(double), st));
+    if (k > 1) {
+        RT_TRY_CUDA(cudaMallocAsync((void**)&lores, nl * sizeof(float), st));
+        RT_TRY_CUDA(cudaMallocAsync((void**)&rmed, nl * sizeof(float), st));
+        k_scrunch<<<dim3((unsigned)std::min<size_t>((nl * 32 + 255) / 256, 4096), 1), 256, 0, st>>>(
+            d_x, A, k, lores);
+        s = launch_running_median(lores, A.lo_len, A.lo_off, 1, nl, w, rmed, st);
+    } else {
+        RT_TRY_CUDA(cudaMallocAsync((void**)&rmed, size * sizeof(float), st));
+        s = launch_running_median(d_x, A.len, A.off, 1, size, w, rmed, st);
+    }
+    if (s == RT_OK) {
+        k_dered<<<dim3(blocks, 1), kStatThreads, 0, st>>>(d_x, A, k, rmed, d_out, part, blocks);
+        s = check_cuda(cudaGetLastError(), "deredden");
+    }
+    if (lores) cudaFreeAsync(lores, st);
+    if (rmed) cudaFreeAsync(rmed, st);
+    cudaFreeAsync(part, st);
+    cudaFreeAsync(d, st);
+    if (s == RT_OK) s = check_cuda(cudaStreamSynchronize(st), "deredden");
+    return s;
+}
+
+extern "C" int rt_normalise(const float* d_x, size_t size, float* d_out, void* stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    if (size == 0) return RT_OK;
+    size_t* d = nullptr;
+    TrialArrays A;
+    RT_TRY(one_series_arrays(size, 0, &d, st, &A));
+    double* part = nullptr;
+    const int blocks = 64;
+    RT_TRY_CUDA(cudaMallocAsync((void**)&part, (blocks * 3 + 2) * sizeof(double), st));
+    double* mean = part + blocks * 3;
+    double* norm = mean + 1;
+    k_sums<<<dim3(blocks, 1), kStatThreads, 0, st>>>(d_x, A, part, blocks);
+    k_stats<<<1, 32, 0, st>>>(part, A.len, blocks, 1, mean, norm);
+    k_normalise<<<dim3(std::max(1, (int)std::min<size_t>((size + 255) / 256, 4096)), 1), 256, 0, st>>>(
+        d_x, A, mean, norm, d_out);
+    int s = check_cuda(cudaGetLastError(), "normalise");
+    cudaFreeAsync(part, st);
+    cudaFreeAsync(d, st);
+    if (s == RT_OK) s = check_cuda(cudaStreamSynchronize(st), "normalise");
+    return s;
+}

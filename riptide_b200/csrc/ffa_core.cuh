@@ -1,0 +1,300 @@
+// FFA transform core: one CTA executes one "tree job" of an FFA transform in shared memory.
+//
+// The reference computes the transform of an m x b block (cpp/transforms.hpp:30-50) by
+// recursive halving: head = rows >> 1 (cpp/block.hpp:30-31), tail = the rest, then
+//     out[s] = head[h] + roll(tail[t], -(s - t)),   h = int(kh*s + .5f), t = int(kt*s + .5f)
+// (transforms.hpp:13-27; the shift h + b_s of the reference equals s - t).
+//
+// Here the recursion tree is cut into jobs that fit one CTA's shared memory:
+//   * a job has a root node (a subtree of the transform: first row, row count), the range of
+//     root output rows it must produce, and a depth G: nodes at depth G below the root are
+//     computed straight from a global source array whose row j holds the output of a node
+//     at depth G+1 (or, for full-depth jobs, raw input row j);
+//   * going down the tree, a contiguous output range of a node needs a contiguous range of
+//     rows of each child, so every level is a list of (node, row range) stored back to back
+//     in a shared-memory buffer; two buffers alternate between levels;
+//   * the root rows are then either written to global memory (to feed a job higher in the
+//     tree, or as the ffa2 result) or turned into boxcar S/N (snr_core.cuh).
+// Additions are float32 and performed in exactly the reference's order, so the result is
+// bit-identical to cpp/transforms.hpp.
+#pragma once
+#include "common.cuh"
+
+namespace rt {
+
+constexpr int kMaxJobDepth = 7;      // levels computed inside one job (<= 128 nodes at the bottom)
+constexpr int kMaxJobNodes = 256;    // total nodes of all levels of one job
+constexpr int kThreads = 512;        // threads per CTA of every FFA kernel
+constexpr int kWarps = kThreads / 32;
+
+struct Node {
+    int row0;   // first row of the node in the transform
+    int rows;   // node size
+    int lo;     // first needed output row (node-local)
+    int hi;     // one past the last needed output row
+    int off;    // row of `lo` inside this level's shared buffer
+};
+
+struct JobTree {
+    Node nodes[kMaxJobNodes];
+    int level_start[kMaxJobDepth + 2];  // index of the first node of each level
+    int level_rows[kMaxJobDepth + 2];   // rows stored for each level
+    int depth;                          // G: nodes at this level read the global source
+    int error;                          // nonzero if the job does not fit
+};
+
+// Description of one job, produced by the planners (host).
+struct JobSpec {
+    int root_row0, root_rows;  // root node
+    int lo, hi;                // root output range
+    int G;                     // relative depth of the level computed from the global source
+};
+
+// Full-depth job: G = smallest depth d with ceil(M / 2^d) <= 2 (all nodes there have 1 or
+// 2 rows, whose children are single input rows).
+RT_HD int full_depth(int rows)
+{
+    int d = 0;
+    while (((rows + (1 << d) - 1) >> d) > 2) ++d;
+    return d;
+}
+
+// Builds the per-level node lists of a job. Called by all threads of the CTA.
+__device__ inline void build_job_tree(JobTree& T, const JobSpec& J, int cap_rows)
+{
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        T.depth = J.G;
+        T.error = (J.G > kMaxJobDepth || (2 << J.G) - 1 > kMaxJobNodes) ? 1 : 0;
+        T.level_start[0] = 0;
+        Node r;
+        r.row0 = J.root_row0;
+        r.rows = J.root_rows;
+        r.lo = J.lo;
+        r.hi = J.hi;
+        r.off = 0;
+        T.nodes[0] = r;
+        T.level_rows[0] = J.hi - J.lo;
+        for (int d = 1; d <= J.G && d <= kMaxJobDepth; ++d) T.level_start[d] = (1 << d) - 1;
+    }
+    __syncthreads();
+    if (T.error) return;
+    for (int d = 0; d < J.G; ++d) {
+        const int n = 1 << d;
+        const int base = T.level_start[d], cbase = T.level_start[d + 1];
+        if (tid < n) {
+            const Node p = T.nodes[base + tid];
+            const int mh = p.rows >> 1, mt = p.rows - mh;
+            Node h, t;
+            h.row0 = p.row0;
+            h.rows = mh;
+            t.row0 = p.row0 + mh;
+            t.rows = mt;
+            if (p.hi > p.lo) {
+                const MergeCoef c = merge_coef(p.rows);
+                h.lo = merge_row(c.kh, p.lo);
+                h.hi = merge_row(c.kh, p.hi - 1) + 1;
+                t.lo = merge_row(c.kt, p.lo);
+                t.hi = merge_row(c.kt, p.hi - 1) + 1;
+            } else {
+                h.lo = h.hi = t.lo = t.hi = 0;
+            }
+            h.off = t.off = 0;
+            T.nodes[cbase + 2 * tid] = h;
+            T.nodes[cbase + 2 * tid + 1] = t;
+        }
+        __syncthreads();
+        // exclusive prefix of row counts -> buffer offsets (2n <= 256 entries)
+        if (tid < 32) {
+            const int cnt = 2 * n;
+            int carry = 0;
+            for (int base2 = 0; base2 < cnt; base2 += 32) {
+                const int i = base2 + tid;
+                int v = (i < cnt) ? (T.nodes[cbase + i].hi - T.nodes[cbase + i].lo) : 0;
+                int incl = v;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (tid >= o) incl += y;
+                }
+                if (i < cnt) T.nodes[cbase + i].off = carry + incl - v;
+                carry += __shfl_sync(0xffffffffu, incl, 31);
+            }
+            if (tid == 0) {
+                T.level_rows[d + 1] = carry;
+                if (carry > cap_rows) T.error = 2;
+            }
+        }
+        __syncthreads();
+    }
+    if (tid == 0 && T.level_rows[0] > cap_rows) T.error = 2;
+    __syncthreads();
+}
+
+// Index of the node holding buffer row r at a level (nodes sorted by `off`).
+__device__ __forceinline__ int find_node(const Node* nodes, int n, int r)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (nodes[mid].off <= r) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// out[c] = head[c] + tail[(c + shift) mod b] for one row, one warp. HeadT/TailT are
+// either shared or global pointers (global ones read through L2 with ld.global.cg).
+template <bool kGlobal>
+__device__ __forceinline__ float ld_src(const float* p)
+{
+    if constexpr (kGlobal) return __ldcg(p);
+    else return *p;
+}
+
+template <bool kGlobal>
+__device__ __forceinline__ void merge_row_warp(const float* __restrict__ head,
+                                               const float* __restrict__ tail, int shift, int b,
+                                               float* __restrict__ dst, int lane)
+{
+    for (int c = lane; c < b; c += 32) {
+        int idx = c + shift;
+        idx -= (idx >= b) ? b : 0;
+        dst[c] = __fadd_rn(ld_src<kGlobal>(head + c), ld_src<kGlobal>(tail + idx));
+    }
+}
+
+template <bool kGlobal>
+__device__ __forceinline__ void copy_row_warp(const float* __restrict__ src, int b,
+                                              float* __restrict__ dst, int lane)
+{
+    for (int c = lane; c < b; c += 32) dst[c] = ld_src<kGlobal>(src + c);
+}
+
+// Runs all levels of the job. On return, the root rows [lo, hi) are in buf[0] (stride
+// `stride`, row i of the buffer = root output row lo + i). `src` is the global source:
+// row j of it is at src + j * b (j in transform row indexing).
+__device__ inline void run_job_levels(const JobTree& T, const float* __restrict__ src, int b,
+                               float* buf0, float* buf1, int stride)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int d = T.depth; d >= 0; --d) {
+        float* dst = (d & 1) ? buf1 : buf0;
+        const float* prev = (d & 1) ? buf0 : buf1;  // level d+1
+        const Node* lvl = T.nodes + T.level_start[d];
+        const int n = 1 << d;
+        const int total = T.level_rows[d];
+        const Node* child = T.nodes + T.level_start[d + 1];
+        for (int r = warp; r < total; r += kWarps) {
+            const int i = find_node(lvl, n, r);
+            const Node nd = lvl[i];
+            const int s = nd.lo + (r - nd.off);
+            float* out = dst + (size_t)r * stride;
+            if (d == T.depth) {
+                // children (or the node itself when it has a single row) live in global memory
+                if (nd.rows == 1) {
+                    copy_row_warp<true>(src + (size_t)nd.row0 * b, b, out, lane);
+                } else {
+                    const MergeCoef c = merge_coef(nd.rows);
+                    const int h = merge_row(c.kh, s), t = merge_row(c.kt, s);
+                    const int mh = nd.rows >> 1;
+                    const int shift = (s - t) % b;
+                    merge_row_warp<true>(src + (size_t)(nd.row0 + h) * b,
+                                         src + (size_t)(nd.row0 + mh + t) * b, shift, b, out,
+                                         lane);
+                }
+            } else {
+                const MergeCoef c = merge_coef(nd.rows);
+                const int h = merge_row(c.kh, s), t = merge_row(c.kt, s);
+                const Node hn = child[2 * i], tn = child[2 * i + 1];
+                const int shift = (s - t) % b;
+                merge_row_warp<false>(prev + (size_t)(hn.off + h - hn.lo) * stride,
+                                      prev + (size_t)(tn.off + t - tn.lo) * stride, shift, b,
+                                      out, lane);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Writes the root rows held in buf0 to global rows (root_row0 + s) of `dst` (stride b).
+__device__ __forceinline__ void store_root_rows(const JobTree& T, const float* buf0, int stride,
+                                                int b, float* __restrict__ dst)
+{
+    const Node r = T.nodes[0];
+    const int nrows = r.hi - r.lo;
+    const int total = nrows * b;
+    float* base = dst + (size_t)(r.row0 + r.lo) * b;
+    for (int i = threadIdx.x; i < total; i += kThreads) {
+        const int row = i / b, c = i - row * b;
+        base[i] = buf0[(size_t)row * stride + c];
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Host-side planning of the stages of one transform.
+//
+// Stage 0 computes nodes at depth D[0] fully (full-depth jobs from the raw rows); stage k
+// computes the needed rows of nodes at depth D[k] from the outputs of depth D[k-1]; the
+// last stage has D = 0 (the root) and produces rows [0, rows_out).
+// ------------------------------------------------------------------------------------
+constexpr int kMaxStages = 4;
+
+struct StagePlan {
+    int nstages;
+    int D[kMaxStages];      // node depth produced by each stage
+    int R[kMaxStages];      // output rows per job (per node) of each stage
+    int jobs[kMaxStages];   // number of jobs of each stage
+    int jobs_per_node[kMaxStages];
+};
+
+// Plans the stages of a transform with m rows whose root output is [0, rows_out), for
+// level buffers of cap_rows rows. Uses the bound: a job whose root range has R rows holds at
+// most R + 3 * 2^G rows at any level (a child range of an L-row range has <= (L + 3) / 2
+// rows, since kh, kt <= 1/2).
+bool plan_stages(int m, int rows_out, int cap_rows, StagePlan* P);
+// Job k of stage s of a transform (host or device).
+RT_HD void node_at(int m, int d, int i, int* row0, int* rows)
+{
+    int r0 = 0, rr = m;
+    for (int k = d - 1; k >= 0; --k) {
+        const int mh = rr >> 1;
+        if ((i >> k) & 1) {
+            r0 += mh;
+            rr -= mh;
+        } else {
+            rr = mh;
+        }
+    }
+    *row0 = r0;
+    *rows = rr;
+}
+
+RT_HD JobSpec stage_job(int m, int rows_out, const StagePlan& P, int stage, int job)
+{
+    JobSpec J;
+    const int d = P.D[stage];
+    if (stage == 0) {
+        int r0, rr;
+        node_at(m, d, job, &r0, &rr);
+        J.root_row0 = r0;
+        J.root_rows = rr;
+        J.lo = 0;
+        J.hi = (P.nstages == 1) ? rows_out : rr;
+        J.G = full_depth(rr);
+        return J;
+    }
+    const int node = job / P.jobs_per_node[stage];
+    const int part = job - node * P.jobs_per_node[stage];
+    int r0, rr;
+    node_at(m, d, node, &r0, &rr);
+    const int hi_node = (stage == P.nstages - 1) ? rows_out : rr;
+    J.root_row0 = r0;
+    J.root_rows = rr;
+    J.lo = part * P.R[stage];
+    J.hi = J.lo + P.R[stage] < hi_node ? J.lo + P.R[stage] : hi_node;
+    J.G = P.D[stage - 1] - d - 1;
+    return J;
+}
+
+}  // namespace rt

@@ -1,0 +1,583 @@
+// Building-block kernels and their host launchers: the drop-ins for the reference's
+// `libcpp` functions (cpp/python_bindings.cpp:44-222) and the plain per-(cycle, bins)
+// periodogram, which issues one launch per step of the reference's loop nest
+// (cpp/periodogram.hpp:153-200). The batched engine (engine.cu) reuses the device code.
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+#include "ffa_core.cuh"
+#include "snr_core.cuh"
+#include "kernels.cuh"
+
+namespace rt {
+
+// ------------------------------------------------------------------------------------
+// Error state
+// ------------------------------------------------------------------------------------
+static thread_local char g_err[512] = "";
+
+int set_error(int code, const char* fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int check_cuda(cudaError_t e, const char* where)
+{
+    if (e == cudaSuccess) return RT_OK;
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        return set_error(RT_ENOMEM, "CUDA out of memory in %s", where);
+    }
+    return set_error(RT_ECUDA, "CUDA error %s (%s) in %s", cudaGetErrorName(e),
+                     cudaGetErrorString(e), where);
+}
+
+const char* last_error() { return g_err; }
+
+// ------------------------------------------------------------------------------------
+// Elementwise helpers (kernels.hpp:19-38, 73-101)
+// ------------------------------------------------------------------------------------
+__global__ void k_rollback(const float* __restrict__ x, size_t size, size_t p,
+                           float* __restrict__ out)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < size;
+         i += (size_t)gridDim.x * blockDim.x) {
+        size_t j = i + p;
+        if (j >= size) j -= size;
+        out[i] = x[j];
+    }
+}
+
+__global__ void k_fused_rollback_add(const float* __restrict__ x, const float* __restrict__ y,
+                                     size_t size, size_t p, float* __restrict__ out)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < size;
+         i += (size_t)gridDim.x * blockDim.x) {
+        size_t j = i + p;
+        if (j >= size) j -= size;
+        out[i] = __fadd_rn(x[i], y[j]);
+    }
+}
+
+static int grid_for(size_t n, int threads)
+{
+    size_t g = (n + threads - 1) / threads;
+    return (int)std::min<size_t>(std::max<size_t>(g, 1), 148 * 32);
+}
+
+int rollback(const float* x, size_t size, size_t shift, float* out, cudaStream_t st)
+{
+    if (size == 0) return RT_OK;
+    k_rollback<<<grid_for(size, 256), 256, 0, st>>>(x, size, shift % size, out);
+    return check_cuda(cudaGetLastError(), "rollback");
+}
+
+int fused_rollback_add(const float* x, const float* y, size_t size, size_t shift, float* out,
+                       cudaStream_t st)
+{
+    if (size == 0) return RT_OK;
+    k_fused_rollback_add<<<grid_for(size, 256), 256, 0, st>>>(x, y, size, shift % size, out);
+    return check_cuda(cudaGetLastError(), "fused_rollback_add");
+}
+
+// One CTA: chunked scan in double of the first min(size, nsum) sums, then the wraps.
+__global__ void k_circular_prefix_sum(const float* __restrict__ x, size_t size, size_t nsum,
+                                      float* __restrict__ out)
+{
+    __shared__ double s_part[1024];
+    __shared__ float s_sumx;
+    const size_t jmax = size < nsum ? size : nsum;
+    const int T = blockDim.x, tid = threadIdx.x;
+    const size_t chunk = (jmax + T - 1) / T;
+    const size_t c0 = std::min(jmax, tid * chunk), c1 = std::min(jmax, c0 + chunk);
+    double local = 0.0;
+    for (size_t c = c0; c < c1; ++c) local += (double)x[c];
+    s_part[tid] = local;
+    __syncthreads();
+    if (tid == 0) {
+        double run = 0.0;
+        for (int i = 0; i < T; ++i) {
+            const double v = s_part[i];
+            s_part[i] = run;
+            run += v;
+        }
+    }
+    __syncthreads();
+    double run = s_part[tid];
+    for (size_t c = c0; c < c1; ++c) {
+        run += (double)x[c];
+        out[c] = __double2float_rn(run);
+    }
+    if (c1 == jmax && c0 < c1) s_sumx = __double2float_rn(run);
+    if (jmax == 0 && tid == 0) s_sumx = 0.f;
+    __syncthreads();
+    if (nsum <= size) return;
+    const float sumx = s_sumx;
+    const size_t q = nsum / size, r = nsum % size;
+    for (size_t i = 1; i < q; ++i)
+        for (size_t j = tid; j < size; j += T)
+            out[i * size + j] = __fadd_rn(out[j], __fmul_rn((float)i, sumx));
+    for (size_t j = tid; j < r; j += T) out[q * size + j] = __fadd_rn(out[j], __fmul_rn((float)q, sumx));
+}
+
+int circular_prefix_sum(const float* x, size_t size, size_t nsum, float* out, cudaStream_t st)
+{
+    if (nsum == 0) return RT_OK;
+    if (size == 0) return set_error(RT_EINVAL, "input array must not be empty");
+    k_circular_prefix_sum<<<1, 1024, 0, st>>>(x, size, nsum, out);
+    return check_cuda(cudaGetLastError(), "circular_prefix_sum");
+}
+
+// ------------------------------------------------------------------------------------
+// FFA stage kernel: one CTA per job; root rows written to dst.
+// ------------------------------------------------------------------------------------
+int ffa_cap_rows(int b)
+{
+    const size_t avail = kFfaSmemBytes - sizeof(JobTree) - 256;
+    const int stride = ffa_stride(b);
+    return (int)(avail / (2 * (size_t)stride * sizeof(float)));
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    k_ffa_stage(const float* __restrict__ src, float* __restrict__ dst, int m, int b,
+                int rows_out, StagePlan P, int stage, int cap_rows, int* err)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    JobTree& T = *reinterpret_cast<JobTree*>(smem);
+    float* buf0 = reinterpret_cast<float*>(smem + ((sizeof(JobTree) + 255) & ~size_t(255)));
+    const int stride = ffa_stride(b);
+    float* buf1 = buf0 + (size_t)cap_rows * stride;
+    const JobSpec J = stage_job(m, rows_out, P, stage, blockIdx.x);
+    if (J.hi <= J.lo) return;
+    build_job_tree(T, J, cap_rows);
+    if (T.error) {
+        if (threadIdx.x == 0) atomicExch(err, RT_EINTERNAL);
+        return;
+    }
+    run_job_levels(T, src, b, buf0, buf1, stride);
+    store_root_rows(T, buf0, stride, b, dst);
+}
+
+bool plan_stages(int m, int rows_out, int cap_rows, StagePlan* P)
+{
+    memset(P, 0, sizeof(*P));
+    if (m <= cap_rows && full_depth(m) <= kMaxJobDepth) {
+        P->nstages = 1;
+        P->D[0] = 0;
+        P->R[0] = rows_out;
+        P->jobs[0] = 1;
+        P->jobs_per_node[0] = 1;
+        return true;
+    }
+    int D = 0;
+    while ((((m + (1 << D) - 1) >> D) > cap_rows) || full_depth((m + (1 << D) - 1) >> D) > kMaxJobDepth) {
+        ++D;
+        if (D > 20) return false;
+    }
+    int ns = 0;
+    P->D[0] = D;
+    P->R[0] = (m + (1 << D) - 1) >> D;
+    P->jobs[0] = 1 << D;
+    P->jobs_per_node[0] = 1;
+    ns = 1;
+    while (D > 0) {
+        if (ns >= kMaxStages) return false;
+        // largest step e such that R = cap - 3 * 2^(e-1) stays >= cap / 2 (at least 1 level)
+        int e = std::min(D, kMaxJobDepth + 1);
+        int R = 0;
+        for (; e >= 1; --e) {
+            R = cap_rows - 3 * (1 << (e - 1));
+            if (R >= cap_rows / 2 || e == 1) break;
+        }
+        if (R < 1) return false;
+        const int Dn = D - e;
+        const int node_rows = (m + (1 << Dn) - 1) >> Dn;
+        const int need = (Dn == 0) ? rows_out : node_rows;
+        P->D[ns] = Dn;
+        P->R[ns] = R;
+        P->jobs_per_node[ns] = std::max(1, (need + R - 1) / R);
+        P->jobs[ns] = P->jobs_per_node[ns] << Dn;
+        ++ns;
+        D = Dn;
+    }
+    P->nstages = ns;
+    return true;
+}
+
+int ffa_transform(const float* in, int m, int b, int rows_out, float* out, float* scratch,
+                  int* d_err, cudaStream_t st)
+{
+    const int cap = ffa_cap_rows(b);
+    StagePlan P;
+    if (cap < 4 || !plan_stages(m, rows_out, cap, &P))
+        return set_error(RT_EINVAL, "FFA transform of %d x %d does not fit the device plan", m, b);
+    RT_TRY_CUDA(cudaFuncSetAttribute(k_ffa_stage, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kFfaSmemBytes));
+    const float* src = in;
+    for (int s = 0; s < P.nstages; ++s) {
+        float* dst = (s == P.nstages - 1) ? out : scratch + (size_t)(s & 1) * m * b;
+        k_ffa_stage<<<P.jobs[s], kThreads, kFfaSmemBytes, st>>>(src, dst, m, b, rows_out, P, s,
+                                                               cap, d_err);
+        RT_TRY_CUDA(cudaGetLastError());
+        src = dst;
+    }
+    return RT_OK;
+}
+
+size_t ffa_scratch_floats(int m, int b)
+{
+    return (m <= ffa_cap_rows(b)) ? 0 : 2 * (size_t)m * b;
+}
+
+// ------------------------------------------------------------------------------------
+// S/N of rows in global memory (snr.hpp:58-65)
+// ------------------------------------------------------------------------------------
+template <int TPR>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_snr2(const float* __restrict__ x, int rows, int b, const int* __restrict__ widths, int nw,
+           int nfast, float stdnoise, float* __restrict__ out, int tile_rows)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    SnrParams& S = *reinterpret_cast<SnrParams*>(smem);
+    float* C = reinterpret_cast<float*>(smem + ((sizeof(SnrParams) + 255) & ~size_t(255)));
+    snr_params_fill(S, widths, nw, nfast, b);
+    const int cs = prefix_stride(b, S.wmax, TPR);
+    for (int r0 = blockIdx.x * tile_rows; r0 < rows; r0 += gridDim.x * tile_rows) {
+        const int nr = min(tile_rows, rows - r0);
+        prefix_rows(x + (size_t)r0 * b, b, nr, b, S.wmax, C, cs);
+        __syncthreads();
+        snr_rows_from_prefix<TPR, 17>(C, cs, nr, b, S, stdnoise, out + (size_t)r0 * nw, nw);
+        __syncthreads();
+    }
+}
+
+int snr_tile_rows(int b, int wmax)
+{
+    const size_t avail = kFfaSmemBytes - ((sizeof(SnrParams) + 255) & ~size_t(255));
+    return (int)(avail / (sizeof(float) * prefix_stride(b, wmax, snr_tpr(b))));
+}
+
+int detect_fast_widths(const int* w, int nw)
+{
+    if (nw < FastWidths10::NW) return 0;
+    for (int k = 0; k < FastWidths10::NW; ++k)
+        if (w[k] != FastWidths10::w(k)) return 0;
+    return FastWidths10::NW;
+}
+
+int snr2(const float* x, size_t rows, size_t cols, const int* d_widths, const int* h_widths,
+         int nw, float stdnoise, float* out, cudaStream_t st)
+{
+    if (rows == 0 || nw == 0) return RT_OK;
+    int wmax = 0;
+    for (int k = 0; k < nw; ++k) wmax = std::max(wmax, h_widths[k]);
+    const int nfast = detect_fast_widths(h_widths, nw);
+    const int tile = std::min<int>(snr_tile_rows((int)cols, wmax), 1024);
+    if (tile < 1) return set_error(RT_EINVAL, "profiles of %zu bins are too long", cols);
+    const int grid = (int)std::min<size_t>((rows + tile - 1) / tile, 148 * 4);
+    if (nw > kMaxWidths) return set_error(RT_EINVAL, "at most %d trial widths are supported", kMaxWidths);
+    const int tpr = snr_tpr((int)cols);
+    if (tpr == 8) {
+        RT_TRY_CUDA(cudaFuncSetAttribute(k_snr2<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kFfaSmemBytes));
+        k_snr2<8><<<grid, kThreads, kFfaSmemBytes, st>>>(x, (int)rows, (int)cols, d_widths, nw,
+                                                         nfast, stdnoise, out, tile);
+    } else {
+        RT_TRY_CUDA(cudaFuncSetAttribute(k_snr2<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kFfaSmemBytes));
+        k_snr2<16><<<grid, kThreads, kFfaSmemBytes, st>>>(x, (int)rows, (int)cols, d_widths, nw,
+                                                          nfast, stdnoise, out, tile);
+    }
+    return check_cuda(cudaGetLastError(), "snr2");
+}
+
+// ------------------------------------------------------------------------------------
+// Downsampling by a real factor (downsample.hpp:44-82).
+//
+// One CTA owns the output samples whose first input sample imin = floor(k f) falls in its
+// segment [seg0, seg0 + kDsSeg). It stages the segment plus a halo in shared memory with
+// an exclusive prefix sum in double, so each output costs O(1):
+//   out[k] = wmin*z[imin] + (P[imax] - P[imin+1]) + wmax*z[imax]
+// with the reference's FP64 sample bounds and float32 edge weights; the sum is formed in
+// double and rounded once. All cycles of a search are produced in the same pass, so the
+// series is read once. Factors with f + 2 > kDsHalo use k_downsample_wide instead.
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ size_t first_k_at_or_after(size_t i0, double f)
+{
+    // smallest k with floor(k * f) >= i0
+    size_t k = (size_t)ceil((double)i0 / f);
+    while (k > 0 && floor((double)(k - 1) * f) >= (double)i0) --k;
+    while (floor((double)k * f) < (double)i0) ++k;
+    return k;
+}
+
+__global__ void __launch_bounds__(512)
+    k_downsample_segments(DsJob job)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* P = reinterpret_cast<double*>(smem);                    // kDsStage + 1
+    float* zs = reinterpret_cast<float*>(P + kDsStage + 1);          // kDsStage
+    __shared__ int s_cnt[kDsMaxCycles + 1];
+    __shared__ size_t s_k0[kDsMaxCycles];
+    __shared__ double s_part[512 / 32];
+
+    const int trial = blockIdx.y;
+    const size_t N = job.lengths[trial];
+    const size_t seg0 = (size_t)blockIdx.x * kDsSeg;
+    if (seg0 >= N) return;
+    const float* z = job.in + job.in_off[trial];
+    const size_t L = std::min<size_t>(kDsStage, N - seg0);
+    const double mean = job.mean ? job.mean[trial] : 0.0;
+    const double inv = job.norm ? job.norm[trial] : 1.0;
+    const bool affine = job.mean != nullptr;
+    float* zout = job.norm_out ? job.norm_out + job.in_off[trial] : nullptr;
+
+    // stage (and optionally normalise) the segment + halo
+    for (size_t i = threadIdx.x; i < L; i += blockDim.x) {
+        float v = __ldg(z + seg0 + i);
+        if (affine) v = __double2float_rn(__ddiv_rn(__dsub_rn((double)v, mean), inv));
+        zs[i] = v;
+        if (zout && i < kDsSeg) zout[seg0 + i] = v;
+    }
+    __syncthreads();
+    // exclusive prefix in double: 512 threads x 16 contiguous elements
+    {
+        const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+        const int per = kDsStage / 512;
+        const int c0 = tid * per;
+        double local = 0.0;
+        for (int j = 0; j < per; ++j) {
+            const int i = c0 + j;
+            local += (i < (int)L) ? (double)zs[i] : 0.0;
+        }
+        double incl = local;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) s_part[warp] = incl;
+        __syncthreads();
+        if (tid == 0) {
+            double run = 0.0;
+            for (int w = 0; w < 512 / 32; ++w) {
+                const double v = s_part[w];
+                s_part[w] = run;
+                run += v;
+            }
+        }
+        __syncthreads();
+        double ex = __shfl_up_sync(0xffffffffu, incl, 1);
+        if (lane == 0) ex = 0.0;
+        double run = s_part[warp] + ex;
+        for (int j = 0; j < per; ++j) {
+            const int i = c0 + j;
+            P[i] = run;
+            run += (i < (int)L) ? (double)zs[i] : 0.0;
+        }
+        if (tid == 511) P[kDsStage] = run;
+    }
+    // outputs per cycle whose imin lies in the segment
+    const size_t seg1 = std::min(N, seg0 + kDsSeg);
+    if (threadIdx.x < job.ncycles) {
+        const int c = threadIdx.x;
+        const double f = job.f[c];
+        const size_t n = downsampled_size(N, f);
+        int cnt = 0;
+        size_t k0 = 0;
+        if (job.use_seg[c] && n > 0) {
+            k0 = first_k_at_or_after(seg0, f);
+            size_t k1 = (seg1 >= N) ? n : first_k_at_or_after(seg1, f);
+            k1 = std::min(k1, n);
+            cnt = k1 > k0 ? (int)(k1 - k0) : 0;
+        }
+        s_cnt[c] = cnt;
+        s_k0[c] = k0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int c = 0; c < job.ncycles; ++c) {
+            const int v = s_cnt[c];
+            s_cnt[c] = run;
+            run += v;
+        }
+        s_cnt[job.ncycles] = run;
+    }
+    __syncthreads();
+    const int total = s_cnt[job.ncycles];
+    for (int q = threadIdx.x; q < total; q += blockDim.x) {
+        int c = 0;
+        while (s_cnt[c + 1] <= q) ++c;
+        const size_t k = s_k0[c] + (q - s_cnt[c]);
+        const double f = job.f[c];
+        const double start = (double)k * f;
+        const double end = start + f;
+        const size_t imin = (size_t)floor(start);
+        const double fe = floor(end);
+        const size_t imax = (size_t)(fe < (double)N - 1.0 ? fe : (double)N - 1.0);
+        const float wmin = __double2float_rn((double)(imin + 1) - start);
+        const float wmax = __double2float_rn(end - (double)imax);
+        const size_t li = imin - seg0, ui = imax - seg0;
+        const double acc = (double)wmin * (double)zs[li] + (P[ui] - P[li + 1]) +
+                           (double)wmax * (double)zs[ui];
+        float* o = job.out + job.out_off[(size_t)trial * job.ncycles + c];
+        o[k] = __double2float_rn(acc);
+    }
+}
+
+// Wide factors: one warp per output sample, deterministic warp tree in double.
+__global__ void k_downsample_wide(DsJob job, int cycle)
+{
+    const int trial = blockIdx.y;
+    const size_t N = job.lengths[trial];
+    const double f = job.f[cycle];
+    const size_t n = downsampled_size(N, f);
+    const float* z = job.in + job.in_off[trial];
+    const double mean = job.mean ? job.mean[trial] : 0.0;
+    const double inv = job.norm ? job.norm[trial] : 1.0;
+    const bool affine = job.mean != nullptr;
+    float* o = job.out + job.out_off[(size_t)trial * job.ncycles + cycle];
+    const int lane = threadIdx.x & 31;
+    const size_t wid = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
+    const size_t nwarp = ((size_t)gridDim.x * blockDim.x) >> 5;
+    for (size_t k = wid; k < n; k += nwarp) {
+        const double start = (double)k * f;
+        const double end = start + f;
+        const size_t imin = (size_t)floor(start);
+        const double fe = floor(end);
+        const size_t imax = (size_t)(fe < (double)N - 1.0 ? fe : (double)N - 1.0);
+        double acc = 0.0;
+        for (size_t i = imin + 1 + lane; i < imax; i += 32) {
+            float v = __ldg(z + i);
+            if (affine) v = __double2float_rn(__ddiv_rn(__dsub_rn((double)v, mean), inv));
+            acc += (double)v;
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+        if (lane == 0) {
+            float a = __ldg(z + imin), bb = __ldg(z + imax);
+            if (affine) {
+                a = __double2float_rn(__ddiv_rn(__dsub_rn((double)a, mean), inv));
+                bb = __double2float_rn(__ddiv_rn(__dsub_rn((double)bb, mean), inv));
+            }
+            const float wmin = __double2float_rn((double)(imin + 1) - start);
+            const float wmax = __double2float_rn(end - (double)imax);
+            o[k] = __double2float_rn((double)wmin * a + acc + (double)wmax * bb);
+        }
+    }
+}
+
+int launch_downsample(const DsJob& job, int ntrials, size_t max_len, cudaStream_t st)
+{
+    bool any_seg = job.norm_out != nullptr;  // the segment pass also writes the normalised copy
+    for (int c = 0; c < job.ncycles; ++c) any_seg |= job.use_seg_host[c] != 0;
+    if (any_seg) {
+        const size_t smem = (kDsStage + 1) * sizeof(double) + kDsStage * sizeof(float);
+        RT_TRY_CUDA(cudaFuncSetAttribute(k_downsample_segments,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        dim3 grid((unsigned)((max_len + kDsSeg - 1) / kDsSeg), (unsigned)ntrials);
+        k_downsample_segments<<<grid, 512, smem, st>>>(job);
+        RT_TRY_CUDA(cudaGetLastError());
+    }
+    for (int c = 0; c < job.ncycles; ++c) {
+        if (job.use_seg_host[c] || job.skip_host[c]) continue;
+        dim3 grid(148 * 2, (unsigned)ntrials);
+        k_downsample_wide<<<grid, 256, 0, st>>>(job, c);
+        RT_TRY_CUDA(cudaGetLastError());
+    }
+    return RT_OK;
+}
+
+// ------------------------------------------------------------------------------------
+// Running median (running_median.hpp:100-132): exact order statistic of rank width/2 of the
+// edge-padded window. Counting selection over a shared-memory tile.
+// ------------------------------------------------------------------------------------
+__global__ void k_running_median(const float* __restrict__ x, const size_t* __restrict__ lengths,
+                                 const size_t* __restrict__ offsets, int width,
+                                 float* __restrict__ out, int tile)
+{
+    extern __shared__ float sx[];
+    const int trial = blockIdx.y;
+    const size_t N = lengths[trial];
+    const float* xr = x + offsets[trial];
+    float* orow = out + offsets[trial];
+    const int half = width / 2;
+    const size_t t0 = (size_t)blockIdx.x * tile;
+    if (t0 >= N) return;
+    const int span = tile + 2 * half;
+    for (int i = threadIdx.x; i < span; i += blockDim.x) {
+        long long g = (long long)t0 + i - half;
+        g = g < 0 ? 0 : (g >= (long long)N ? (long long)N - 1 : g);
+        sx[i] = xr[g];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < tile; i += blockDim.x) {
+        const size_t gi = t0 + i;
+        if (gi >= N) break;
+        const float* win = sx + i;
+        float med = win[0];
+        for (int j = 0; j < width; ++j) {
+            const float cand = win[j];
+            int less = 0, leq = 0;
+            for (int q = 0; q < width; ++q) {
+                const float v = win[q];
+                less += v < cand;
+                leq += v <= cand;
+            }
+            if (less <= half && half < leq) {
+                med = cand;
+                break;
+            }
+        }
+        orow[gi] = med;
+    }
+}
+
+int launch_running_median(const float* x, const size_t* d_lengths, const size_t* d_offsets,
+                          int ntrials, size_t max_len, int width, float* out, cudaStream_t st)
+{
+    int tile = 256;
+    size_t smem = (tile + width) * sizeof(float);
+    if (smem > kFfaSmemBytes)
+        return set_error(RT_EINVAL, "running median width %d is larger than supported", width);
+    if (smem > 48 * 1024)
+        RT_TRY_CUDA(cudaFuncSetAttribute(k_running_median,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid((unsigned)((max_len + tile - 1) / tile), (unsigned)ntrials);
+    k_running_median<<<grid, 256, smem, st>>>(x, d_lengths, d_offsets, width, out, tile);
+    return check_cuda(cudaGetLastError(), "running_median");
+}
+
+// ------------------------------------------------------------------------------------
+// Trial periods / fold bins of one transform (periodogram.hpp:190-194)
+// ------------------------------------------------------------------------------------
+__global__ void k_periods(double* __restrict__ periods, uint32_t* __restrict__ foldbins,
+                          size_t rows_eval, double tau, int bins, size_t rows)
+{
+    for (size_t s = blockIdx.x * (size_t)blockDim.x + threadIdx.x; s < rows_eval;
+         s += (size_t)gridDim.x * blockDim.x) {
+        periods[s] = trial_period(tau, bins, s, rows);
+        foldbins[s] = (uint32_t)bins;
+    }
+}
+
+int launch_periods(double* periods, uint32_t* foldbins, size_t rows_eval, double tau, int bins,
+                   size_t rows, cudaStream_t st)
+{
+    if (rows_eval == 0) return RT_OK;
+    k_periods<<<grid_for(rows_eval, 256), 256, 0, st>>>(periods, foldbins, rows_eval, tau, bins,
+                                                        rows);
+    return check_cuda(cudaGetLastError(), "periods");
+}
+
+}  // namespace rt

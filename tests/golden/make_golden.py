@@ -1,0 +1,198 @@
+"""Generate the golden fixtures in this folder from the REFERENCE implementation itself.
+
+Run in a container where the reference project is mounted (default /root/reference,
+override with RIPTIDE_REF_ROOT):
+
+    make -C oracle ref            # the reference's libcpp, built from its own sources
+    python tests/golden/make_golden.py
+
+What it runs: the reference's compiled ``libcpp`` (oracle/_ref) for the C++ kernels, and the
+reference's own Python glue (src/riptide/{search,time_series,running_medians,libffa,
+ffautils}.py) imported from the reference tree. The glue imports matplotlib, astropy and
+schema, which are not installed here; they are replaced by inert stand-ins that none of
+the code paths exercised below call (plotting, sky coordinates, metadata validation).
+
+Inputs are seeded (numpy default_rng); every input is stored beside its output, so the
+tests need neither the reference nor this script at run time.
+"""
+import os
+import sys
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+REF_ROOT = os.environ.get("RIPTIDE_REF_ROOT", "/root/reference")
+sys.path.insert(0, REPO)
+
+
+def _install_stubs():
+    class _Anything:
+        def __init__(self, *a, **k):
+            self.schema = a[0] if a else None
+
+        def __call__(self, *a, **k):
+            return _Anything()
+
+        def __getattr__(self, name):
+            return _Anything()
+
+        def validate(self, x):
+            return x
+
+    def mod(name, **attrs):
+        m = types.ModuleType(name)
+        m.__dict__.update(attrs)
+        m.__getattr__ = lambda n: _Anything()
+        sys.modules[name] = m
+        return m
+
+    mpl = mod("matplotlib")
+    mpl.pyplot = mod("matplotlib.pyplot")
+    ap = mod("astropy")
+    ap.units = mod("astropy.units")
+    ap.coordinates = mod("astropy.coordinates", SkyCoord=type("SkyCoord", (), {}))
+    mod("schema", Schema=_Anything, And=_Anything, Or=_Anything, Optional=_Anything)
+
+
+def import_reference():
+    """Import the reference package `riptide` from REF_ROOT with the compiled libcpp."""
+    from oracle import oracle as O
+
+    libcpp = O.ref_libcpp()
+    if libcpp is None:
+        raise SystemExit("reference libcpp missing: run `make -C oracle ref` first")
+    _install_stubs()
+    pkg = types.ModuleType("riptide")
+    pkg.__path__ = [os.path.join(REF_ROOT, "src", "riptide")]
+    sys.modules["riptide"] = pkg
+    sys.modules["riptide.libcpp"] = libcpp
+    pkg.libcpp = libcpp
+    import importlib
+
+    mods = {}
+    for name in ("timing", "ffautils", "libffa", "running_medians", "time_series", "search"):
+        mods[name] = importlib.import_module("riptide." + name)
+    return libcpp, mods
+
+
+def main():
+    libcpp, M = import_reference()
+    rng = np.random.default_rng(20240531)
+    out = {}
+
+    # --- ffa2: bit-exact target -------------------------------------------------------
+    shapes = [(1, 5), (2, 3), (3, 7), (4, 4), (5, 241), (7, 2), (8, 8), (9, 260), (13, 17),
+              (16, 33), (31, 250), (64, 64), (100, 241), (257, 13)]
+    ffa_in, ffa_out = [], []
+    for m, b in shapes:
+        x = rng.standard_normal((m, b)).astype(np.float32)
+        ffa_in.append(x.ravel())
+        ffa_out.append(libcpp.ffa2(x).ravel())
+    np.savez_compressed(
+        os.path.join(HERE, "ffa2.npz"), shapes=np.array(shapes, dtype=np.int64),
+        inputs=np.concatenate(ffa_in), outputs=np.concatenate(ffa_out))
+
+    # --- snr2 ----------------------------------------------------------------------------
+    snr_cases = []
+    for rows, cols, widths, stdnoise in [
+        (50, 240, M["ffautils"].generate_width_trials(240), 1.0),
+        (40, 260, M["ffautils"].generate_width_trials(240), 3.25),
+        (20, 480, M["ffautils"].generate_width_trials(480), 1.0),
+        (10, 64, np.arange(1, 64), 0.5),
+        (5, 7, np.array([1, 2, 3, 6]), 2.0),
+    ]:
+        x = (rng.standard_normal((rows, cols)) * 5 + 0.5).astype(np.float32)
+        w = np.asarray(widths, dtype=np.uint64)
+        snr_cases.append((x, w, stdnoise, libcpp.snr2(x, w, stdnoise)))
+    np.savez_compressed(
+        os.path.join(HERE, "snr2.npz"),
+        **{f"x{i}": c[0] for i, c in enumerate(snr_cases)},
+        **{f"w{i}": c[1] for i, c in enumerate(snr_cases)},
+        **{f"s{i}": np.float64(c[2]) for i, c in enumerate(snr_cases)},
+        **{f"y{i}": c[3] for i, c in enumerate(snr_cases)},
+        n=len(snr_cases))
+
+    # --- downsample --------------------------------------------------------------------
+    ds = {}
+    x = rng.standard_normal(20011).astype(np.float32) + 0.25
+    factors = [1.5, 2.0, 3.0, 7.25, 13.020833333333334, 20.833333333333332, 97.5, 1000.0,
+               20011.0 / 7.0, 20011.0]
+    for i, f in enumerate(factors):
+        ds[f"y{i}"] = libcpp.downsample(x, f)
+    np.savez_compressed(os.path.join(HERE, "downsample.npz"), x=x,
+                        factors=np.array(factors), **ds, n=len(factors))
+
+    # --- running median: bit-exact target ------------------------------------------------
+    x = rng.standard_normal(3001).astype(np.float32)
+    x[100:140] = 0.5  # ties
+    widths = [1, 3, 5, 7, 11, 25, 37, 101, 999]
+    rm = {f"y{w}": libcpp.running_median(x, w) for w in widths}
+    np.savez_compressed(os.path.join(HERE, "running_median.npz"), x=x,
+                        widths=np.array(widths), **rm)
+
+    # --- periodogram on a small series (reference libcpp) --------------------------------
+    x = rng.standard_normal(1 << 14).astype(np.float32)
+    pg_cfgs = [
+        # tsamp, pmin, pmax, bmin, bmax
+        (1e-3, 0.5, 5.0, 240, 260),
+        (1e-3, 0.24, 0.6, 240, 260),   # first cycle at f == 1 (no downsampling)
+        (4e-4, 0.3, 3.0, 100, 120),
+        (5e-4, 0.25, 9.0, 480, 520),
+    ]
+    pg = {}
+    for i, (tsamp, pmin, pmax, bmin, bmax) in enumerate(pg_cfgs):
+        w = M["ffautils"].generate_width_trials(bmin).astype(np.uint64)
+        p, fb, s = libcpp.periodogram(x, tsamp, w, pmin, pmax, bmin, bmax)
+        pg[f"p{i}"], pg[f"fb{i}"], pg[f"s{i}"], pg[f"w{i}"] = p, fb, s, w
+    np.savez_compressed(os.path.join(HERE, "periodogram.npz"), x=x,
+                        cfgs=np.array(pg_cfgs, dtype=np.float64), **pg, n=len(pg_cfgs))
+
+    # --- ffa_search end to end through the reference's own Python glue ------------------
+    TS = M["time_series"].TimeSeries
+    ffa_search = M["search"].ffa_search
+    fs = {}
+    cases = [
+        # nsamp, tsamp, period(s), amplitude, kwargs
+        (1 << 15, 1e-3, 1.0, 20.0, dict(period_min=0.5, period_max=5.0, rmed_width=4.0)),
+        (20000, 5e-4, 0.37, 15.0, dict(period_min=0.2, period_max=2.0, rmed_width=1.0,
+                                       rmed_minpts=51)),
+        (15000, 1e-3, 1.3, 12.0, dict(period_min=0.8, period_max=2.0, deredden=False)),
+    ]
+    for i, (nsamp, tsamp, period, amp, kw) in enumerate(cases):
+        crng = np.random.default_rng(1000 + i)
+        t = np.arange(nsamp) / (period / tsamp)
+        kappa = np.log(2.0) / (2.0 * np.sin(np.pi * 0.03 / 2.0) ** 2)
+        sig = np.exp(kappa * (np.cos(2 * np.pi * (t - 0.5)) - 1.0))
+        sig *= amp / np.sqrt((sig ** 2).sum())
+        data = (sig + crng.standard_normal(nsamp) + 0.3 * np.sin(np.arange(nsamp) * 2e-4)
+                + 3.0).astype(np.float32)
+        ts = TS(data, tsamp)
+        tsdr, pgram = ffa_search(ts, **kw)
+        fs[f"x{i}"] = data
+        fs[f"tsamp{i}"] = np.float64(tsamp)
+        fs[f"z{i}"] = tsdr.data
+        fs[f"p{i}"], fs[f"fb{i}"], fs[f"s{i}"] = pgram.periods, pgram.foldbins, pgram.snrs
+        fs[f"w{i}"] = np.asarray(pgram.widths)
+        for k, v in kw.items():
+            fs[f"kw{i}_{k}"] = np.asarray(v)
+    np.savez_compressed(os.path.join(HERE, "ffa_search.npz"), **fs, n=len(cases))
+
+    # --- glue pieces: deredden / normalise / fast_running_median -------------------------
+    x = (rng.standard_normal(30000) + np.linspace(0, 5, 30000)).astype(np.float32)
+    g = {"x": x}
+    g["norm"] = TS(x, 1e-3).normalise().data
+    g["dered_w0.5_m51"] = TS(x, 1e-3).deredden(0.5, minpts=51).data
+    g["dered_w4_m101"] = TS(x, 1e-3).deredden(4.0, minpts=101).data
+    g["frm_w2001_m101"] = M["running_medians"].fast_running_median(x, 2001, 101)
+    g["frm_w37_m41"] = M["running_medians"].fast_running_median(x, 37, 41)
+    np.savez_compressed(os.path.join(HERE, "glue.npz"), **g)
+
+    for f in sorted(os.listdir(HERE)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(HERE, f)))
+
+
+if __name__ == "__main__":
+    main()

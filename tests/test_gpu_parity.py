@@ -1,0 +1,254 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle and the reference's golden
+fixtures. Tolerances: FFA transform, running median, periods and fold bins are bit-exact;
+S/N is bit-exact when its inputs are identical; downsampling and everything downstream of it
+(the reference reorders that float sum) within rtol 1e-5 plus an absolute floor."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from test_oracle_pins import FFA_IN_88, FFA_OUT_88
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def rb():
+    import riptide_b200
+
+    return riptide_b200
+
+
+# ------------------------------------------------------------------------------ FFA
+def test_ffa2_known_answer(rb):
+    for shift in range(8):
+        X = np.roll(FFA_IN_88, shift, axis=1)
+        assert np.array_equal(rb.ffa2(X), np.roll(FFA_OUT_88, shift, axis=1))
+        assert np.array_equal(rb.ffa1(X.ravel(), 8), np.roll(FFA_OUT_88, shift, axis=1))
+    for extra in range(8):
+        X = np.hstack([FFA_IN_88, np.zeros((8, extra), np.float32)])
+        truth = np.hstack([FFA_OUT_88, np.zeros((8, extra), np.float32)])
+        assert np.array_equal(rb.ffa2(X), truth)
+
+
+def test_ffa2_errors(rb):
+    with pytest.raises(ValueError):
+        rb.ffa2(np.zeros(4))
+    with pytest.raises(ValueError):
+        rb.ffa1(np.zeros((4, 4)), 4)
+    with pytest.raises(ValueError):
+        rb.ffa1(np.zeros(10), 11)
+    with pytest.raises(ValueError):
+        rb.ffa1(np.zeros(10), 4.0)
+    with pytest.raises(ValueError, match="contiguous"):
+        rb.libcpp.ffa2(np.zeros((8, 8), np.float32)[:, ::2])
+
+
+def test_ffa2_golden(rb, golden):
+    g = golden("ffa2.npz")
+    off = 0
+    for m, b in g["shapes"]:
+        n = int(m * b)
+        x = g["inputs"][off:off + n].reshape(m, b)
+        assert np.array_equal(rb.libcpp.ffa2(x), g["outputs"][off:off + n].reshape(m, b)), (m, b)
+        off += n
+
+
+@pytest.mark.parametrize("m,b", [(1, 7), (2, 240), (3, 260), (63, 241), (107, 260), (108, 259),
+                                 (150, 250), (511, 240), (1342, 240), (1241, 260), (2684, 480),
+                                 (1290, 520), (5000, 61), (20000, 3), (257, 1000)])
+def test_ffa2_random_bit_exact(rb, m, b):
+    x = np.random.default_rng(m * 1000 + b).standard_normal((m, b)).astype(np.float32)
+    assert np.array_equal(rb.libcpp.ffa2(x), O.C().ffa2(x))
+
+
+def test_ffa2_device_tensor(rb):
+    import torch
+
+    x = np.random.default_rng(1).standard_normal((300, 251)).astype(np.float32)
+    t = torch.from_numpy(x).cuda()
+    y = rb.libcpp.ffa2(t)
+    assert y.is_cuda and np.array_equal(y.cpu().numpy(), O.C().ffa2(x))
+
+
+# ------------------------------------------------------------------------------ S/N
+def test_snr2_golden_bit_exact(rb, golden):
+    g = golden("snr2.npz")
+    for i in range(int(g["n"])):
+        y = rb.libcpp.snr2(g[f"x{i}"], g[f"w{i}"], float(g[f"s{i}"]))
+        assert np.array_equal(y, g[f"y{i}"]), i
+
+
+@pytest.mark.parametrize("b,widths", [
+    (240, O.generate_width_trials(240)), (260, O.generate_width_trials(240)),
+    (251, O.generate_width_trials(251)), (480, O.generate_width_trials(480)),
+    (520, O.generate_width_trials(480)), (300, O.generate_width_trials(300, ducy_max=0.3)),
+    (64, np.arange(1, 64)), (33, [1, 5, 7, 32]), (1000, [3, 30, 300])])
+def test_snr2_random_bit_exact(rb, b, widths):
+    x = (np.random.default_rng(b).standard_normal((777, b)) * 4).astype(np.float32)
+    y = rb.libcpp.snr2(x, widths, 1.75)
+    assert np.array_equal(y, O.C().snr2(x, widths, 1.75))
+
+
+def test_snr_properties(rb):
+    # tests/test_snr.py of the reference: errors, shapes, phase-roll invariance, top hat
+    data = np.zeros(32, dtype="float32")
+    for bad in ([0, 1], [1, 32]):
+        with pytest.raises(ValueError):
+            rb.boxcar_snr(data, bad)
+    with pytest.raises(ValueError):
+        rb.boxcar_snr(data, [1, 2], stdnoise=-42.0)
+    w = [1, 2, 3, 5]
+    assert rb.boxcar_snr(np.zeros(32, np.float32), w).shape == (4,)
+    assert rb.boxcar_snr(np.zeros((4, 32), np.float32), w).shape == (4, 4)
+    assert rb.boxcar_snr(np.zeros((3, 4, 32), np.float32), w).shape == (3, 4, 4)
+    d = np.random.default_rng(2).normal(size=(4, 32)).astype("float32")
+    ref = rb.boxcar_snr(d, [1, 2, 5, 11, 18, 31])
+    for shift in range(1, 33):
+        assert np.allclose(rb.boxcar_snr(np.roll(d, shift, axis=-1), [1, 2, 5, 11, 18, 31]), ref)
+    n = 64
+    data = np.zeros(n, dtype="float32")
+    for width in range(1, n):
+        data[:width] = 1.0
+        snr = rb.boxcar_snr(data, np.arange(1, n))
+        assert snr.argmax() == width - 1
+        assert np.allclose(snr.max(), width * np.sqrt((n - width) / (n * width)))
+
+
+# ------------------------------------------------------------------------------ downsample
+def test_downsample_golden_and_oracle(rb, golden):
+    g = golden("downsample.npz")
+    x = g["x"]
+    for i, f in enumerate(g["factors"]):
+        y = rb.downsample(x, float(f))
+        assert y.shape == g[f"y{i}"].shape
+        assert np.allclose(y, g[f"y{i}"], rtol=1e-5, atol=1e-6 * np.sqrt(f)), f
+        y64 = O.C().downsample(x.astype(np.float64), float(f), f64=True)
+        assert np.max(np.abs(y - y64)) <= 1e-6 * max(1.0, np.abs(y64).max()), f
+
+
+def test_downsample_wide_and_errors(rb):
+    x = np.random.default_rng(9).standard_normal(200003).astype(np.float32)
+    for f in [4093.5, 5000.0, 12345.678, 200003.0]:
+        y = rb.downsample(x, f)
+        assert np.allclose(y, O.C().downsample(x, f), rtol=1e-5, atol=1e-6 * np.sqrt(f))
+    for f in [0.55, 1.0, 200004.0]:
+        with pytest.raises(ValueError, match="Downsampling factor"):
+            rb.downsample(x, f)
+
+
+# ------------------------------------------------------------------------------ running median
+def test_running_median(rb, golden):
+    g = golden("running_median.npz")
+    for w in g["widths"]:
+        assert np.array_equal(rb.running_median(g["x"], int(w)), g[f"y{w}"]), w
+    data = np.random.default_rng(4).normal(size=300).reshape(100, 3).astype("float32")
+    for col in data.T:  # non-contiguous column slices
+        for w in [1, 3, 5, 7, 11, 25, 37]:
+            assert np.array_equal(rb.running_median(col, w), O.C().running_median(col, w))
+    d10 = np.arange(10, dtype="float32")
+    for args in [(d10, 2), (d10, 10), (d10[:9], 9), (np.zeros((4, 8)), 3)]:
+        with pytest.raises(ValueError):
+            rb.running_median(*args)
+
+
+def test_fast_running_median_noscrunch(rb):
+    x = np.random.default_rng(5).normal(size=100)
+    for w in [1, 3, 5, 7, 11, 25, 37]:
+        assert np.array_equal(rb.running_median(x, w), rb.fast_running_median(x, w, min_points=39))
+    with pytest.raises(ValueError):
+        rb.fast_running_median(np.zeros(100), 3, min_points=10)
+
+
+# ------------------------------------------------------------------------------ glue
+def test_normalise_deredden_golden(rb, golden):
+    g = golden("glue.npz")
+    ts = rb.TimeSeries(g["x"], 1e-3)
+    assert np.allclose(ts.normalise().data, g["norm"], rtol=1e-6, atol=1e-6)
+    assert np.allclose(ts.deredden(0.5, minpts=51).data, g["dered_w0.5_m51"], rtol=1e-5, atol=1e-5)
+    assert np.allclose(ts.deredden(4.0, minpts=101).data, g["dered_w4_m101"], rtol=1e-5, atol=1e-5)
+    assert np.allclose(rb.fast_running_median(g["x"], 2001, 101), g["frm_w2001_m101"],
+                       rtol=1e-5, atol=1e-5)
+    tc = rb.TimeSeries(np.full(10000, 42.42, np.float32), 1e-3)
+    assert np.allclose(tc.deredden(0.5, minpts=51).data, 0.0, atol=1e-5)
+
+
+# ------------------------------------------------------------------------------ periodogram
+def _check_pgram(p, fb, s, p_ref, fb_ref, s_ref, rtol=1e-5, atol=2e-5):
+    assert np.array_equal(p, p_ref)
+    assert np.array_equal(fb, fb_ref)
+    assert s.shape == s_ref.shape
+    assert np.allclose(s, s_ref, rtol=rtol, atol=atol)
+    assert np.argmax(s.max(axis=1)) == np.argmax(s_ref.max(axis=1))
+    assert np.argmax(s.max(axis=0)) == np.argmax(s_ref.max(axis=0))
+
+
+def test_periodogram_golden(rb, golden):
+    g = golden("periodogram.npz")
+    for i, (tsamp, pmin, pmax, bmin, bmax) in enumerate(g["cfgs"]):
+        args = (g["x"], tsamp, g[f"w{i}"], pmin, pmax, int(bmin), int(bmax))
+        out = rb.libcpp.periodogram(*args)
+        _check_pgram(*out, g[f"p{i}"], g[f"fb{i}"], g[f"s{i}"])
+        plain = rb.libcpp.periodogram_plain(*args)
+        for a, b in zip(out, plain):
+            assert np.array_equal(a, b)
+
+
+def test_periodogram_config1_full_size(rb):
+    # 2^20 samples, 100 us, P 0.5-5 s, bins 240-260: the reference's own C++ when built here
+    rng = np.random.default_rng(100000)
+    x = rb.generate_signal(1 << 20, 1.0 / 1e-4, ducy=0.02, amplitude=20.0, rng=rng)
+    x = O.normalise(x)
+    w = O.generate_width_trials(240)
+    R = O.ref_libcpp()
+    ref = (R.periodogram(x, 1e-4, w.astype(np.uint64), 0.5, 5.0, 240, 260) if R is not None
+           else O.C().periodogram(x, 1e-4, w, 0.5, 5.0, 240, 260))
+    out = rb.libcpp.periodogram(x, 1e-4, w, 0.5, 5.0, 240, 260)
+    _check_pgram(*out, *ref)
+
+
+def test_periodogram_empty_is_an_error_like_the_reference(rb):
+    with pytest.raises(IndexError):
+        rb.libcpp.periodogram(np.zeros(200, np.float32), 1e-3, [1, 2], 0.24, 60.0, 240, 260)
+
+
+def test_ffa_search_golden(rb, golden):
+    g = golden("ffa_search.npz")
+    for i in range(int(g["n"])):
+        kw = {k.split("_", 1)[1]: g[k].item() for k in g if k.startswith(f"kw{i}_")}
+        ts = rb.TimeSeries(g[f"x{i}"], float(g[f"tsamp{i}"]))
+        tsdr, pg = rb.ffa_search(ts, **kw)
+        assert np.allclose(tsdr.data, g[f"z{i}"], rtol=1e-5, atol=1e-5)
+        assert np.array_equal(pg.widths, g[f"w{i}"])
+        _check_pgram(pg.periods, pg.foldbins, pg.snrs, g[f"p{i}"], g[f"fb{i}"], g[f"s{i}"],
+                     rtol=1e-4, atol=1e-4)
+    ts = rb.TimeSeries(g["x0"], float(g["tsamp0"]))
+    tsdr, pg = rb.ffa_search(ts, period_min=0.5, period_max=5.0, deredden=False,
+                             already_normalised=True)
+    assert tsdr is ts  # search.py:41-50 of the reference tests
+
+
+# ------------------------------------------------------------------------------ batched
+def test_batched_equals_single(rb):
+    rng = np.random.default_rng(77)
+    lengths = [70001, 65536, 90000, 50000, 81234]
+    series = [rb.generate_signal(n, 0.9 / 5e-4 + 13 * i, ducy=0.04, amplitude=15.0, rng=rng)
+              .astype(np.float32) + 0.5 for i, n in enumerate(lengths)]
+    kw = dict(period_min=0.2, period_max=3.0, bins_min=240, bins_max=260, rmed_width=1.0)
+    pgs = rb.ffa_search_batched(series, 5e-4, **kw)
+    for s, pg in zip(series, pgs):
+        tsdr, one = rb.ffa_search(rb.TimeSeries(s, 5e-4), **kw)
+        assert np.array_equal(pg.snrs, one.snrs)
+        assert np.array_equal(pg.periods, one.periods)
+        z, widths, p, fb, sn = O.ffa_search(s, 5e-4, **kw)
+        _check_pgram(pg.periods, pg.foldbins, pg.snrs, p, fb, sn, rtol=1e-4, atol=1e-4)
+
+
+def test_batched_full_size_trial(rb):
+    # one 2^22-sample trial at the batched configuration, against the oracle
+    rng = np.random.default_rng(300007)
+    x = rb.generate_signal(1 << 22, 0.731 / 64e-6, ducy=0.03, amplitude=25.0, rng=rng).astype(np.float32)
+    pgs, zs = rb.BatchedSearch([x.size], 64e-6, period_min=0.2, period_max=30.0).search(
+        [x], return_normalised=True)
+    z, widths, p, fb, sn = O.ffa_search(x, 64e-6, period_min=0.2, period_max=30.0)
+    assert np.allclose(zs[0], z, rtol=1e-5, atol=1e-5)
+    _check_pgram(pgs[0].periods, pgs[0].foldbins, pgs[0].snrs, p, fb, sn, rtol=1e-4, atol=1e-4)
