@@ -46,6 +46,8 @@ SIGNATURES = {
     "rt_search_check": (ctypes.c_int, [_vp, _vp]),
     "rt_search_set_timing": (ctypes.c_int, [_vp, ctypes.c_int]),
     "rt_search_last_timing": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int)]),
+    "rt_search_set_profiling": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "rt_search_phase_cycles": (ctypes.c_int, [_vp, _u64p, ctypes.c_int]),
     "rt_search_plan_destroy": (None, [_vp]),
 }
 

@@ -125,6 +125,18 @@ class BatchedSearch(object):
         _lib.check(_lib.load().rt_search_last_timing(self._plan, ms, ctypes.byref(n)))
         return float(ms[0]), float(ms[1]), float(ms[2]), int(n.value)
 
+    def enable_profiling(self, enable=True):
+        """Accumulate per-phase SM cycles inside the persistent kernel (see phase_cycles)."""
+        _lib.check(_lib.load().rt_search_set_profiling(self._plan, int(bool(enable))))
+
+    def phase_cycles(self, reset=True):
+        """{phase: summed SM cycles} of the runs since the last reset."""
+        c = np.zeros(8, dtype=np.uint64)
+        _lib.check(_lib.load().rt_search_phase_cycles(self._plan, c.ctypes.data_as(_lib._u64p),
+                                                      int(bool(reset))))
+        names = ["fetch", "wait", "tree", "levels", "snr", "store"]
+        return {n: int(c[i]) for i, n in enumerate(names)}
+
     def close(self):
         if getattr(self, "_plan", None):
             _lib.load().rt_search_plan_destroy(self._plan)

@@ -45,9 +45,10 @@ struct WorkItem {
 // Shared-memory layout of the persistent kernel: job tree, S/N parameters, two level buffers.
 constexpr size_t kEngineTreeBytes = (sizeof(JobTree) + 255) & ~size_t(255);
 constexpr size_t kEngineSnrBytes = (sizeof(SnrParams) + 255) & ~size_t(255);
-constexpr size_t kEngineBufFloats =
-    (kFfaSmemBytes - kEngineTreeBytes - kEngineSnrBytes) / (2 * sizeof(float));
-RT_HD int engine_cap_rows(int b) { return (int)(kEngineBufFloats / ffa_stride(b)); }
+RT_HD int engine_cap_rows(int b)
+{
+    return ffa_cap_rows_for(kFfaSmemBytes, kEngineTreeBytes + kEngineSnrBytes, b);
+}
 
 constexpr int kSlots = 16;           // scratch slots for multi-stage transforms
 constexpr int kPipelineLag = 2;      // stage s of transform i follows stage 0 of i + s*lag
@@ -71,7 +72,11 @@ struct EngineArgs {
     int* slot_release;       // [kSlots]
     unsigned long long* ticket;
     int* error;              // RT_OK or an error code
+    unsigned long long* phase_cycles;  // optional [kPhases] SM-cycle totals (thread 0 of each CTA)
 };
+
+// Phases of one work item, for the optional in-kernel profile.
+enum { kPhFetch = 0, kPhWait, kPhTree, kPhLevels, kPhSnr, kPhStore, kPhases = 8 };
 
 __device__ __forceinline__ int ld_acquire(const int* p)
 {
@@ -126,12 +131,22 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_persistent(EngineArgs A)
     extern __shared__ __align__(16) unsigned char smem[];
     JobTree& T = *reinterpret_cast<JobTree*>(smem);
     SnrParams& S = *reinterpret_cast<SnrParams*>(smem + kEngineTreeBytes);
-    float* bufs = reinterpret_cast<float*>(smem + kEngineTreeBytes + kEngineSnrBytes);
+    unsigned char* layout = smem + kEngineTreeBytes + kEngineSnrBytes;
     __shared__ long long s_item;
     __shared__ int s_ok;
     __shared__ int s_b;
     if (threadIdx.x == 0) s_b = -1;
 
+    const bool prof = A.phase_cycles != nullptr;
+    unsigned long long ph[kPhases] = {0, 0, 0, 0, 0, 0, 0, 0};
+    long long tprev = prof ? clock64() : 0;
+    auto mark = [&](int phase) {
+        if (prof && threadIdx.x == 0) {
+            const long long t = clock64();
+            ph[phase] += (unsigned long long)(t - tprev);
+            tprev = t;
+        }
+    };
     for (;;) {
         if (threadIdx.x == 0) {
             s_item = (ld_acquire(A.error) != RT_OK) ? A.nitems
@@ -149,10 +164,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_persistent(EngineArgs A)
         const int b = X.b;
         const int fstride = ffa_stride(b);
         const int cap_rows = engine_cap_rows(b);
-        float* buf0 = bufs;
-        float* buf1 = bufs + (size_t)cap_rows * fstride;
+        const FfaSmem L = ffa_smem(layout, cap_rows, b);
+        float* buf0 = L.buf0;
+        float* buf1 = L.buf1;
         float* slot = (X.seq >= 0) ? A.scratch + (size_t)(X.seq % kSlots) * 2 * A.slot_floats
                                    : nullptr;
+        mark(kPhFetch);
         if (threadIdx.x == 0) {
             s_ok = 1;
             if (J.hi > J.lo && X.seq >= 0) {
@@ -172,6 +189,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_persistent(EngineArgs A)
             if (threadIdx.x == 0) s_b = b;
         }
         __syncthreads();
+        mark(kPhWait);
         if (!s_ok) break;
         if (J.hi > J.lo) {
             const float* src =
@@ -182,12 +200,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_persistent(EngineArgs A)
                 if (threadIdx.x == 0) atomicExch(A.error, RT_EINTERNAL);
                 break;
             }
-            run_job_levels(T, src, b, buf0, buf1, fstride);
+            mark(kPhTree);
+            run_job_levels(T, src, b, buf0, buf1, fstride, L.ops);
+            mark(kPhLevels);
             if (last) {
                 if (snr_tpr(b) == 8)
                     final_stage_outputs<8>(T, X, A, S, buf0, buf1, fstride, cap_rows);
                 else
                     final_stage_outputs<16>(T, X, A, S, buf0, buf1, fstride, cap_rows);
+                mark(kPhSnr);
             } else {
                 store_root_rows(T, buf0, fstride, b, slot + (size_t)(stage & 1) * A.slot_floats);
             }
@@ -202,7 +223,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_persistent(EngineArgs A)
                 atomicAdd(A.slot_release + (X.seq % kSlots), 1);
             }
         }
+        mark(kPhStore);
     }
+    if (prof && threadIdx.x == 0)
+        for (int i = 0; i < kPhases; ++i) atomicAdd(A.phase_cycles + i, ph[i]);
 }
 
 // ------------------------------------------------------------------------------------
@@ -474,6 +498,7 @@ struct SearchPlan {
     // optional per-stage CUDA-event timing: deredden+normalise, downsample, FFA + S/N
     bool timing = false;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    unsigned long long* d_phase = nullptr;  // in-kernel phase profile (optional)
     int launches_last_run = 0;
 };
 
@@ -804,6 +829,7 @@ static int plan_run(SearchPlan& P, const float* data, float* normalised_out, dou
     A.slot_release = P.d_counters + (size_t)P.nseq * kMaxStages;
     A.error = A.slot_release + kSlots;
     A.ticket = P.d_ticket;
+    A.phase_cycles = P.d_phase;
     RT_TRY_CUDA(cudaFuncSetAttribute(k_search_persistent,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)kFfaSmemBytes));
@@ -946,10 +972,36 @@ extern "C" int rt_search_last_timing(rt_search_plan* plan, float* h_ms, int* h_l
     return RT_OK;
 }
 
+extern "C" int rt_search_set_profiling(rt_search_plan* plan, int enable)
+{
+    if (!plan) return set_error(RT_EINVAL, "null argument");
+    SearchPlan& P = plan->p;
+    if (enable && !P.d_phase) {
+        RT_TRY_CUDA(cudaMalloc((void**)&P.d_phase, kPhases * sizeof(unsigned long long)));
+        RT_TRY_CUDA(cudaMemset(P.d_phase, 0, kPhases * sizeof(unsigned long long)));
+    } else if (!enable && P.d_phase) {
+        cudaFree(P.d_phase);
+        P.d_phase = nullptr;
+    }
+    return RT_OK;
+}
+
+extern "C" int rt_search_phase_cycles(rt_search_plan* plan, uint64_t* h_cycles, int reset)
+{
+    if (!plan || !h_cycles) return set_error(RT_EINVAL, "null argument");
+    SearchPlan& P = plan->p;
+    if (!P.d_phase) return set_error(RT_EINVAL, "profiling is not enabled on this plan");
+    RT_TRY_CUDA(cudaDeviceSynchronize());
+    RT_TRY_CUDA(cudaMemcpy(h_cycles, P.d_phase, kPhases * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    if (reset) RT_TRY_CUDA(cudaMemset(P.d_phase, 0, kPhases * sizeof(unsigned long long)));
+    return RT_OK;
+}
+
 extern "C" void rt_search_plan_destroy(rt_search_plan* plan)
 {
     if (!plan) return;
     cudaDeviceSynchronize();
+    if (plan->p.d_phase) cudaFree(plan->p.d_phase);
     for (int i = 0; i < 4; ++i)
         if (plan->p.ev[i]) cudaEventDestroy(plan->p.ev[i]);
     plan_free_device(plan->p);

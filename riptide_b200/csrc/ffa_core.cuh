@@ -143,76 +143,162 @@ __device__ __forceinline__ int find_node(const Node* nodes, int n, int r)
     return lo;
 }
 
-// out[c] = head[c] + tail[(c + shift) mod b] for one row, one warp. HeadT/TailT are
-// either shared or global pointers (global ones read through L2 with ld.global.cg).
-template <bool kGlobal>
-__device__ __forceinline__ float ld_src(const float* p)
+// Rows in shared memory carry a wrap halo: columns [b, b + kHalo) repeat columns
+// [0, kHalo), so a warp reading 32 consecutive columns of a rolled row never wraps
+// (used when b >= kHalo).
+constexpr int kHalo = 32;
+RT_HD int ffa_stride(int b) { return (b + kHalo + 3) & ~3; }
+
+// One output row of a level: out = row h + roll(row t, -shift) of the level below.
+// For the level read from global memory, h and t are global row indices; t < 0 marks a
+// single-row node (out = row h).
+struct RowOp {
+    int h, t, shift;
+};
+
+// Builds the row operations of level d (one thread per output row).
+__device__ __forceinline__ void build_level_ops(const JobTree& T, int d, int b, RowOp* ops)
 {
-    if constexpr (kGlobal) return __ldcg(p);
-    else return *p;
+    const Node* lvl = T.nodes + T.level_start[d];
+    const Node* child = T.nodes + T.level_start[d + 1];
+    const int n = 1 << d;
+    const int total = T.level_rows[d];
+    for (int r = threadIdx.x; r < total; r += blockDim.x) {
+        const int i = find_node(lvl, n, r);
+        const Node nd = lvl[i];
+        const int s = nd.lo + (r - nd.off);
+        RowOp op;
+        if (nd.rows == 1) {
+            op.h = nd.row0;
+            op.t = -1;
+            op.shift = 0;
+        } else {
+            const MergeCoef c = merge_coef(nd.rows);
+            const int h = merge_row(c.kh, s), t = merge_row(c.kt, s);
+            op.shift = (s - t) % b;
+            if (d == T.depth) {
+                op.h = nd.row0 + h;
+                op.t = nd.row0 + (nd.rows >> 1) + t;
+            } else {
+                const Node hn = child[2 * i], tn = child[2 * i + 1];
+                op.h = hn.off + h - hn.lo;
+                op.t = tn.off + t - tn.lo;
+            }
+        }
+        ops[r] = op;
+    }
 }
 
-template <bool kGlobal>
-__device__ __forceinline__ void merge_row_warp(const float* __restrict__ head,
-                                               const float* __restrict__ tail, int shift, int b,
-                                               float* __restrict__ dst, int lane)
+// Computes the rows of one level, one warp per row. NIT = ceil(b / 32) when kUnroll.
+// kGlobal: operands are rows of the global source (packed, stride b, no halo).
+template <int NIT, bool kGlobal>
+__device__ __forceinline__ void level_rows_unrolled(const RowOp* ops, int nrows,
+                                                    const float* __restrict__ src, int sstride,
+                                                    float* __restrict__ dst, int stride, int b)
 {
-    for (int c = lane; c < b; c += 32) {
-        int idx = c + shift;
-        idx -= (idx >= b) ? b : 0;
-        dst[c] = __fadd_rn(ld_src<kGlobal>(head + c), ld_src<kGlobal>(tail + idx));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int r = warp; r < nrows; r += kWarps) {
+        const RowOp op = ops[r];
+        float* out = dst + (size_t)r * stride;
+        const float* H = src + (size_t)op.h * sstride;
+        float v[NIT];
+        if (op.t < 0) {
+#pragma unroll
+            for (int j = 0; j < NIT; ++j) {
+                const int c = lane + 32 * j;
+                if (j < NIT - 1 || c < b) v[j] = kGlobal ? __ldcg(H + c) : H[c];
+            }
+        } else {
+            const float* Tr = src + (size_t)op.t * sstride;
+#pragma unroll
+            for (int j = 0; j < NIT; ++j) {
+                const int c = lane + 32 * j;
+                if (j < NIT - 1 || c < b) {
+                    int base = 32 * j + op.shift;
+                    base -= (base >= b) ? b : 0;
+                    if constexpr (kGlobal) {
+                        int idx = base + lane;
+                        idx -= (idx >= b) ? b : 0;
+                        v[j] = __fadd_rn(__ldcg(H + c), __ldcg(Tr + idx));
+                    } else {
+                        v[j] = __fadd_rn(H[c], Tr[base + lane]);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < NIT; ++j) {
+            const int c = lane + 32 * j;
+            if (j < NIT - 1 || c < b) out[c] = v[j];
+        }
+        out[b + lane] = v[0];  // halo (b >= 32 on this path)
+    }
+}
+
+// Any b: per-element wrap, no unrolling (b < 32 or b > 32 * 17).
+template <bool kGlobal>
+__device__ __forceinline__ void level_rows_generic(const RowOp* ops, int nrows,
+                                                   const float* __restrict__ src, int sstride,
+                                                   float* __restrict__ dst, int stride, int b)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int r = warp; r < nrows; r += kWarps) {
+        const RowOp op = ops[r];
+        float* out = dst + (size_t)r * stride;
+        const float* H = src + (size_t)op.h * sstride;
+        const float* Tr = src + (size_t)(op.t < 0 ? 0 : op.t) * sstride;
+        for (int c = lane; c < b; c += 32) {
+            float v;
+            if (op.t < 0) {
+                v = kGlobal ? __ldcg(H + c) : H[c];
+            } else {
+                int idx = c + op.shift;
+                idx -= (idx >= b) ? b : 0;
+                v = kGlobal ? __fadd_rn(__ldcg(H + c), __ldcg(Tr + idx)) : __fadd_rn(H[c], Tr[idx]);
+            }
+            out[c] = v;
+        }
+        __syncwarp();
+        if (b >= kHalo) out[b + lane] = out[lane];
+        __syncwarp();
     }
 }
 
 template <bool kGlobal>
-__device__ __forceinline__ void copy_row_warp(const float* __restrict__ src, int b,
-                                              float* __restrict__ dst, int lane)
+__device__ __forceinline__ void level_rows(const RowOp* ops, int nrows, const float* src,
+                                           int sstride, float* dst, int stride, int b)
 {
-    for (int c = lane; c < b; c += 32) dst[c] = ld_src<kGlobal>(src + c);
+    const int nit = (b + 31) >> 5;
+    if (b < kHalo) {
+        level_rows_generic<kGlobal>(ops, nrows, src, sstride, dst, stride, b);
+        return;
+    }
+    switch (nit) {
+#define RT_NIT_CASE(N) \
+    case N: level_rows_unrolled<N, kGlobal>(ops, nrows, src, sstride, dst, stride, b); break;
+        // bins 225-288 and 449-544 cover the usual searches (bins_min 240 / 480)
+        RT_NIT_CASE(8) RT_NIT_CASE(9) RT_NIT_CASE(15) RT_NIT_CASE(16) RT_NIT_CASE(17)
+#undef RT_NIT_CASE
+        default: level_rows_generic<kGlobal>(ops, nrows, src, sstride, dst, stride, b);
+    }
 }
 
-// Runs all levels of the job. On return, the root rows [lo, hi) are in buf[0] (stride
+// Runs all levels of the job. On return, the root rows [lo, hi) are in buf0 (stride
 // `stride`, row i of the buffer = root output row lo + i). `src` is the global source:
-// row j of it is at src + j * b (j in transform row indexing).
+// row j of it is at src + j * b (j in transform row indexing). `ops` has room for the
+// largest level.
 __device__ inline void run_job_levels(const JobTree& T, const float* __restrict__ src, int b,
-                               float* buf0, float* buf1, int stride)
+                                      float* buf0, float* buf1, int stride, RowOp* ops)
 {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int d = T.depth; d >= 0; --d) {
         float* dst = (d & 1) ? buf1 : buf0;
         const float* prev = (d & 1) ? buf0 : buf1;  // level d+1
-        const Node* lvl = T.nodes + T.level_start[d];
-        const int n = 1 << d;
-        const int total = T.level_rows[d];
-        const Node* child = T.nodes + T.level_start[d + 1];
-        for (int r = warp; r < total; r += kWarps) {
-            const int i = find_node(lvl, n, r);
-            const Node nd = lvl[i];
-            const int s = nd.lo + (r - nd.off);
-            float* out = dst + (size_t)r * stride;
-            if (d == T.depth) {
-                // children (or the node itself when it has a single row) live in global memory
-                if (nd.rows == 1) {
-                    copy_row_warp<true>(src + (size_t)nd.row0 * b, b, out, lane);
-                } else {
-                    const MergeCoef c = merge_coef(nd.rows);
-                    const int h = merge_row(c.kh, s), t = merge_row(c.kt, s);
-                    const int mh = nd.rows >> 1;
-                    const int shift = (s - t) % b;
-                    merge_row_warp<true>(src + (size_t)(nd.row0 + h) * b,
-                                         src + (size_t)(nd.row0 + mh + t) * b, shift, b, out,
-                                         lane);
-                }
-            } else {
-                const MergeCoef c = merge_coef(nd.rows);
-                const int h = merge_row(c.kh, s), t = merge_row(c.kt, s);
-                const Node hn = child[2 * i], tn = child[2 * i + 1];
-                const int shift = (s - t) % b;
-                merge_row_warp<false>(prev + (size_t)(hn.off + h - hn.lo) * stride,
-                                      prev + (size_t)(tn.off + t - tn.lo) * stride, shift, b,
-                                      out, lane);
-            }
-        }
+        build_level_ops(T, d, b, ops);
+        __syncthreads();
+        if (d == T.depth)
+            level_rows<true>(ops, T.level_rows[d], src, b, dst, stride, b);
+        else
+            level_rows<false>(ops, T.level_rows[d], prev, stride, dst, stride, b);
         __syncthreads();
     }
 }
@@ -229,6 +315,30 @@ __device__ __forceinline__ void store_root_rows(const JobTree& T, const float* b
         const int row = i / b, c = i - row * b;
         base[i] = buf0[(size_t)row * stride + c];
     }
+}
+
+// Shared-memory layout of a CTA running FFA jobs: [fixed part][ops][buf0][buf1].
+// Rows per level buffer for `smem_bytes` with `fixed_bytes` already used.
+RT_HD int ffa_cap_rows_for(size_t smem_bytes, size_t fixed_bytes, int b)
+{
+    const size_t per_row = 2 * (size_t)ffa_stride(b) * sizeof(float) + sizeof(RowOp);
+    return (int)((smem_bytes - fixed_bytes - 64) / per_row);
+}
+
+struct FfaSmem {
+    RowOp* ops;
+    float* buf0;
+    float* buf1;
+};
+
+__device__ __forceinline__ FfaSmem ffa_smem(unsigned char* base, int cap_rows, int b)
+{
+    FfaSmem L;
+    L.ops = reinterpret_cast<RowOp*>(base);
+    size_t off = ((size_t)cap_rows * sizeof(RowOp) + 63) & ~size_t(63);
+    L.buf0 = reinterpret_cast<float*>(base + off);
+    L.buf1 = L.buf0 + (size_t)cap_rows * ffa_stride(b);
+    return L;
 }
 
 // ------------------------------------------------------------------------------------

@@ -140,12 +140,9 @@ int circular_prefix_sum(const float* x, size_t size, size_t nsum, float* out, cu
 // ------------------------------------------------------------------------------------
 // FFA stage kernel: one CTA per job; root rows written to dst.
 // ------------------------------------------------------------------------------------
-int ffa_cap_rows(int b)
-{
-    const size_t avail = kFfaSmemBytes - sizeof(JobTree) - 256;
-    const int stride = ffa_stride(b);
-    return (int)(avail / (2 * (size_t)stride * sizeof(float)));
-}
+constexpr size_t kStageTreeBytes = (sizeof(JobTree) + 255) & ~size_t(255);
+
+int ffa_cap_rows(int b) { return ffa_cap_rows_for(kFfaSmemBytes, kStageTreeBytes, b); }
 
 __global__ void __launch_bounds__(kThreads, 1)
     k_ffa_stage(const float* __restrict__ src, float* __restrict__ dst, int m, int b,
@@ -153,9 +150,8 @@ __global__ void __launch_bounds__(kThreads, 1)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     JobTree& T = *reinterpret_cast<JobTree*>(smem);
-    float* buf0 = reinterpret_cast<float*>(smem + ((sizeof(JobTree) + 255) & ~size_t(255)));
+    const FfaSmem L = ffa_smem(smem + kStageTreeBytes, cap_rows, b);
     const int stride = ffa_stride(b);
-    float* buf1 = buf0 + (size_t)cap_rows * stride;
     const JobSpec J = stage_job(m, rows_out, P, stage, blockIdx.x);
     if (J.hi <= J.lo) return;
     build_job_tree(T, J, cap_rows);
@@ -163,8 +159,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (threadIdx.x == 0) atomicExch(err, RT_EINTERNAL);
         return;
     }
-    run_job_levels(T, src, b, buf0, buf1, stride);
-    store_root_rows(T, buf0, stride, b, dst);
+    run_job_levels(T, src, b, L.buf0, L.buf1, stride, L.ops);
+    store_root_rows(T, L.buf0, stride, b, dst);
 }
 
 bool plan_stages(int m, int rows_out, int cap_rows, StagePlan* P)
@@ -220,6 +216,8 @@ int ffa_transform(const float* in, int m, int b, int rows_out, float* out, float
     StagePlan P;
     if (cap < 4 || !plan_stages(m, rows_out, cap, &P))
         return set_error(RT_EINVAL, "FFA transform of %d x %d does not fit the device plan", m, b);
+    if (P.nstages > 1 && scratch == nullptr)
+        return set_error(RT_EINTERNAL, "FFA transform of %d x %d needs scratch memory", m, b);
     RT_TRY_CUDA(cudaFuncSetAttribute(k_ffa_stage, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)kFfaSmemBytes));
     const float* src = in;
@@ -235,7 +233,10 @@ int ffa_transform(const float* in, int m, int b, int rows_out, float* out, float
 
 size_t ffa_scratch_floats(int m, int b)
 {
-    return (m <= ffa_cap_rows(b)) ? 0 : 2 * (size_t)m * b;
+    // multi-stage plans (too many rows, or too deep for one job) need two scratch copies
+    StagePlan P;
+    if (!plan_stages(m, m, ffa_cap_rows(b), &P) || P.nstages == 1) return 0;
+    return 2 * (size_t)m * b;
 }
 
 // ------------------------------------------------------------------------------------

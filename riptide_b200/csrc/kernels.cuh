@@ -8,9 +8,6 @@ namespace rt {
 // Dynamic shared memory of the FFA / S/N kernels (one CTA per SM).
 constexpr size_t kFfaSmemBytes = 220 * 1024;
 
-// Row stride of FFA level buffers (16-byte aligned rows).
-RT_HD int ffa_stride(int b) { return (b + 3) & ~3; }
-
 int ffa_cap_rows(int b);
 size_t ffa_scratch_floats(int m, int b);
 int detect_fast_widths(const int* w, int nw);
