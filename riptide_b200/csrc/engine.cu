@@ -16,6 +16,8 @@
 #include <algorithm>
 #include <deque>
 #include <map>
+#include <set>
+#include <tuple>
 #include <vector>
 
 #include "common.cuh"
@@ -50,8 +52,8 @@ RT_HD int engine_cap_rows(int b)
     return ffa_cap_rows_for(kFfaSmemBytes, kEngineTreeBytes + kEngineSnrBytes, b);
 }
 
-constexpr int kSlots = 16;           // scratch slots for multi-stage transforms
-constexpr int kPipelineLag = 2;      // stage s of transform i follows stage 0 of i + s*lag
+constexpr int kSlots = 48;           // scratch slots for multi-stage transforms
+constexpr size_t kLagItems = 640;    // work items emitted between two stages of a transform
 constexpr long long kSpinLimit = 20000000LL;  // bounded waits (about 2-20 s with backoff)
 
 struct EngineArgs {
@@ -108,16 +110,9 @@ __device__ void final_stage_outputs(const JobTree& T, const XformRec& X, const E
     const Node r = T.nodes[0];
     const int b = X.b;
     const int cs = prefix_stride(b, S.wmax, TPR);
-    const int crows = (int)(((size_t)cap_rows * fstride) / cs);
-    float* snr_out = A.snrs + (size_t)X.out_row * S.nw;
-    for (int c0 = 0; c0 < r.hi - r.lo; c0 += crows) {
-        const int nr = min(crows, r.hi - r.lo - c0);
-        prefix_rows(buf0 + (size_t)c0 * fstride, fstride, nr, b, S.wmax, buf1, cs);
-        __syncthreads();
-        snr_rows_from_prefix<TPR, 17>(buf1, cs, nr, b, S, X.stdnoise,
-                                      snr_out + (size_t)(r.lo + c0) * S.nw, S.nw);
-        __syncthreads();
-    }
+    const int groups = (int)(((size_t)cap_rows * fstride) / cs);
+    snr_rows<TPR, 34>(buf0, fstride, r.hi - r.lo, b, S, X.stdnoise,
+                      A.snrs + ((size_t)X.out_row + r.lo) * S.nw, S.nw, buf1, cs, groups);
     double* per_out = A.periods + X.out_row;
     uint32_t* fb_out = A.foldbins + X.out_row;
     for (int s = r.lo + threadIdx.x; s < r.hi; s += blockDim.x) {
@@ -531,9 +526,10 @@ static int plan_cycles(SearchPlan& P)
     return RT_OK;
 }
 
-// Emits the work items of all transforms. Order: (trial, cycle, bins); for a transform that
-// needs several stages, stage s is emitted after the stage-0 jobs of kPipelineLag * s further
-// multi-stage transforms, so that its wait usually finds the previous stage complete.
+// Emits the work items of all transforms. Order: (trial, cycle, bins). For a transform that
+// needs several stages, stage s + 1 is emitted at least kLagItems items after stage s, so that
+// by the time a CTA takes it the previous stage has usually completed; the transform that
+// reuses a scratch slot starts only after every stage of the previous occupant is emitted.
 static int plan_build(SearchPlan& P)
 {
     RT_TRY(plan_cycles(P));
@@ -543,15 +539,39 @@ static int plan_build(SearchPlan& P)
     P.out_rows_off.assign(T + 1, 0);
     P.ds_off.assign((size_t)T * C, 0);
     std::map<std::pair<int, long long>, int> plan_index;
-    struct Deferred {
-        int xform, stage, due;
-    };
-    std::deque<Deferred> deferred;
-    int stage0_count = 0;
+    std::set<std::tuple<size_t, int, int>> deferred;  // (due item count, xform, stage)
+    std::vector<int> seq_xform;                        // xform of each multi-stage sequence
+    std::vector<std::tuple<size_t, int, int>> seq_pending;  // its deferred entry, if any
+    std::vector<char> seq_has_pending;
 
     auto emit_stage = [&](int xi, int stage) {
         const StagePlan& sp = P.plans[P.xforms[xi].plan];
         for (int j = 0; j < sp.jobs[stage]; ++j) P.items.push_back({xi, (stage << 24) | j});
+        const int seq = P.xforms[xi].seq;
+        if (seq >= 0) {
+            if (stage + 1 < sp.nstages) {
+                auto e = std::make_tuple(P.items.size() + kLagItems, xi, stage + 1);
+                deferred.insert(e);
+                seq_pending[seq] = e;
+                seq_has_pending[seq] = 1;
+            } else {
+                seq_has_pending[seq] = 0;
+            }
+        }
+    };
+    auto flush = [&]() {
+        while (!deferred.empty() && std::get<0>(*deferred.begin()) <= P.items.size()) {
+            const auto e = *deferred.begin();
+            deferred.erase(deferred.begin());
+            emit_stage(std::get<1>(e), std::get<2>(e));
+        }
+    };
+    auto finish_seq = [&](int seq) {  // emit all remaining stages of `seq` now
+        while (seq_has_pending[seq]) {
+            const auto e = seq_pending[seq];
+            deferred.erase(e);
+            emit_stage(std::get<1>(e), std::get<2>(e));
+        }
     };
 
     size_t ds_total = 0;
@@ -591,6 +611,7 @@ static int plan_build(SearchPlan& P)
                 }
                 XformRec X;
                 memset(&X, 0, sizeof(X));
+                const bool multi = P.plans[pi].nstages > 1;
                 X.src_off = (f != 1) ? P.ds_off[(size_t)t * C + ci] : P.offsets[t];
                 X.src_norm = (f != 1) ? 0 : 1;
                 X.out_row = P.out_rows_off[t] + rows_total;
@@ -602,37 +623,28 @@ static int plan_build(SearchPlan& P)
                 X.plan = pi;
                 X.seq = -1;
                 const int xi = (int)P.xforms.size();
-                const StagePlan& sp = P.plans[pi];
-                if (sp.nstages > 1) {
+                if (multi) {
                     X.seq = P.nseq++;
                     P.slot_floats = std::max(P.slot_floats, rows * b);
+                    seq_xform.push_back(xi);
+                    seq_pending.emplace_back();
+                    seq_has_pending.push_back(0);
+                    if (X.seq >= kSlots) finish_seq(X.seq - kSlots);
                 }
                 P.xforms.push_back(X);
                 rows_total += re;
                 emit_stage(xi, 0);
-                if (sp.nstages > 1) {
-                    ++stage0_count;
-                    for (int s = 1; s < sp.nstages; ++s)
-                        deferred.push_back({xi, s, stage0_count + s * kPipelineLag});
-                    std::stable_sort(deferred.begin(), deferred.end(),
-                                     [](const Deferred& a, const Deferred& b2) { return a.due < b2.due; });
-                    while (!deferred.empty() && deferred.front().due <= stage0_count) {
-                        emit_stage(deferred.front().xform, deferred.front().stage);
-                        deferred.pop_front();
-                    }
-                }
+                flush();
             }
         }
         P.out_rows_off[t + 1] = P.out_rows_off[t] + rows_total;
     }
     while (!deferred.empty()) {
-        emit_stage(deferred.front().xform, deferred.front().stage);
-        deferred.pop_front();
+        const auto e = *deferred.begin();
+        deferred.erase(deferred.begin());
+        emit_stage(std::get<1>(e), std::get<2>(e));
     }
     P.ds_total = ds_total;
-    // The slot of sequence q is reused by q + kSlots; all items of q precede the stage-0 items
-    // of q + kSlots in the work order because kSlots > (kMaxStages - 1) * kPipelineLag + 1.
-    static_assert(kSlots > (kMaxStages - 1) * kPipelineLag + 1, "slot ring too small");
 
     // deredden geometry (time_series.py:119, running_medians.py:72-80)
     P.lo_len.assign(T, 0);

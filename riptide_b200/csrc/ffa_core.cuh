@@ -24,7 +24,7 @@ namespace rt {
 
 constexpr int kMaxJobDepth = 7;      // levels computed inside one job (<= 128 nodes at the bottom)
 constexpr int kMaxJobNodes = 256;    // total nodes of all levels of one job
-constexpr int kThreads = 512;        // threads per CTA of every FFA kernel
+constexpr int kThreads = 512;        // threads per CTA of every FFA kernel (1 CTA per SM)
 constexpr int kWarps = kThreads / 32;
 
 struct Node {
@@ -39,6 +39,7 @@ struct JobTree {
     Node nodes[kMaxJobNodes];
     int level_start[kMaxJobDepth + 2];  // index of the first node of each level
     int level_rows[kMaxJobDepth + 2];   // rows stored for each level
+    int op_start[kMaxJobDepth + 2];     // first row operation of each level
     int depth;                          // G: nodes at this level read the global source
     int error;                          // nonzero if the job does not fit
 };
@@ -59,75 +60,84 @@ RT_HD int full_depth(int rows)
     return d;
 }
 
-// Builds the per-level node lists of a job. Called by all threads of the CTA.
+// Builds the per-level node lists of a job (all threads of the CTA, 3 barriers).
+// Node q of the flat array is node i = q - (2^d - 1) of level d; its row range follows from
+// the root range by applying the head/tail row maps along the bits of i.
 __device__ inline void build_job_tree(JobTree& T, const JobSpec& J, int cap_rows)
 {
     const int tid = threadIdx.x;
+    const int G = J.G;
+    const bool bad = (G > kMaxJobDepth || (2 << G) - 1 > kMaxJobNodes);
     if (tid == 0) {
-        T.depth = J.G;
-        T.error = (J.G > kMaxJobDepth || (2 << J.G) - 1 > kMaxJobNodes) ? 1 : 0;
-        T.level_start[0] = 0;
-        Node r;
-        r.row0 = J.root_row0;
-        r.rows = J.root_rows;
-        r.lo = J.lo;
-        r.hi = J.hi;
-        r.off = 0;
-        T.nodes[0] = r;
-        T.level_rows[0] = J.hi - J.lo;
-        for (int d = 1; d <= J.G && d <= kMaxJobDepth; ++d) T.level_start[d] = (1 << d) - 1;
+        T.depth = G;
+        T.error = bad ? 1 : 0;
+    }
+    if (bad) {
+        __syncthreads();
+        return;
+    }
+    const int nnodes = (2 << G) - 1;
+    for (int q = tid; q < nnodes; q += blockDim.x) {
+        const int d = 31 - __clz(q + 1);
+        const int i = q + 1 - (1 << d);
+        int row0 = J.root_row0, rows = J.root_rows, lo = J.lo, hi = J.hi;
+        for (int k = d - 1; k >= 0; --k) {
+            const int mh = rows >> 1;
+            const MergeCoef c = merge_coef(rows);
+            if ((i >> k) & 1) {
+                const int nlo = merge_row(c.kt, lo), nhi = merge_row(c.kt, hi - 1) + 1;
+                row0 += mh;
+                rows -= mh;
+                lo = nlo;
+                hi = nhi;
+            } else {
+                const int nlo = merge_row(c.kh, lo), nhi = merge_row(c.kh, hi - 1) + 1;
+                rows = mh;
+                lo = nlo;
+                hi = nhi;
+            }
+        }
+        Node nd;
+        nd.row0 = row0;
+        nd.rows = rows;
+        nd.lo = lo;
+        nd.hi = hi;
+        nd.off = 0;
+        T.nodes[q] = nd;
+    }
+    if (tid <= G) T.level_start[tid] = (1 << tid) - 1;
+    __syncthreads();
+    // one warp per level: exclusive prefix of the row counts -> buffer offsets
+    const int warp = tid >> 5, lane = tid & 31;
+    if (warp <= G) {
+        const int d = warp, n = 1 << d, base = (1 << d) - 1;
+        int carry = 0;
+        for (int b0 = 0; b0 < n; b0 += 32) {
+            const int i = b0 + lane;
+            const int v = (i < n) ? (T.nodes[base + i].hi - T.nodes[base + i].lo) : 0;
+            int incl = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (i < n) T.nodes[base + i].off = carry + incl - v;
+            carry += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        if (lane == 0) {
+            T.level_rows[d] = carry;
+            if (carry > cap_rows) T.error = 2;
+        }
     }
     __syncthreads();
-    if (T.error) return;
-    for (int d = 0; d < J.G; ++d) {
-        const int n = 1 << d;
-        const int base = T.level_start[d], cbase = T.level_start[d + 1];
-        if (tid < n) {
-            const Node p = T.nodes[base + tid];
-            const int mh = p.rows >> 1, mt = p.rows - mh;
-            Node h, t;
-            h.row0 = p.row0;
-            h.rows = mh;
-            t.row0 = p.row0 + mh;
-            t.rows = mt;
-            if (p.hi > p.lo) {
-                const MergeCoef c = merge_coef(p.rows);
-                h.lo = merge_row(c.kh, p.lo);
-                h.hi = merge_row(c.kh, p.hi - 1) + 1;
-                t.lo = merge_row(c.kt, p.lo);
-                t.hi = merge_row(c.kt, p.hi - 1) + 1;
-            } else {
-                h.lo = h.hi = t.lo = t.hi = 0;
-            }
-            h.off = t.off = 0;
-            T.nodes[cbase + 2 * tid] = h;
-            T.nodes[cbase + 2 * tid + 1] = t;
+    if (tid == 0) {
+        int acc = 0;
+        for (int d = 0; d <= G; ++d) {
+            T.op_start[d] = acc;
+            acc += T.level_rows[d];
         }
-        __syncthreads();
-        // exclusive prefix of row counts -> buffer offsets (2n <= 256 entries)
-        if (tid < 32) {
-            const int cnt = 2 * n;
-            int carry = 0;
-            for (int base2 = 0; base2 < cnt; base2 += 32) {
-                const int i = base2 + tid;
-                int v = (i < cnt) ? (T.nodes[cbase + i].hi - T.nodes[cbase + i].lo) : 0;
-                int incl = v;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (tid >= o) incl += y;
-                }
-                if (i < cnt) T.nodes[cbase + i].off = carry + incl - v;
-                carry += __shfl_sync(0xffffffffu, incl, 31);
-            }
-            if (tid == 0) {
-                T.level_rows[d + 1] = carry;
-                if (carry > cap_rows) T.error = 2;
-            }
-        }
-        __syncthreads();
+        T.op_start[G + 1] = acc;
     }
-    if (tid == 0 && T.level_rows[0] > cap_rows) T.error = 2;
     __syncthreads();
 }
 
@@ -143,11 +153,8 @@ __device__ __forceinline__ int find_node(const Node* nodes, int n, int r)
     return lo;
 }
 
-// Rows in shared memory carry a wrap halo: columns [b, b + kHalo) repeat columns
-// [0, kHalo), so a warp reading 32 consecutive columns of a rolled row never wraps
-// (used when b >= kHalo).
-constexpr int kHalo = 32;
-RT_HD int ffa_stride(int b) { return (b + kHalo + 3) & ~3; }
+// Row stride of the level buffers (16-byte aligned rows).
+RT_HD int ffa_stride(int b) { return (b + 3) & ~3; }
 
 // One output row of a level: out = row h + roll(row t, -shift) of the level below.
 // For the level read from global memory, h and t are global row indices; t < 0 marks a
@@ -156,41 +163,49 @@ struct RowOp {
     int h, t, shift;
 };
 
-// Builds the row operations of level d (one thread per output row).
-__device__ __forceinline__ void build_level_ops(const JobTree& T, int d, int b, RowOp* ops)
+// Row operation of buffer row r of level d.
+__device__ __forceinline__ RowOp make_row_op(const JobTree& T, int d, int r, int b)
 {
     const Node* lvl = T.nodes + T.level_start[d];
-    const Node* child = T.nodes + T.level_start[d + 1];
-    const int n = 1 << d;
-    const int total = T.level_rows[d];
-    for (int r = threadIdx.x; r < total; r += blockDim.x) {
-        const int i = find_node(lvl, n, r);
-        const Node nd = lvl[i];
-        const int s = nd.lo + (r - nd.off);
-        RowOp op;
-        if (nd.rows == 1) {
-            op.h = nd.row0;
-            op.t = -1;
-            op.shift = 0;
+    const int i = find_node(lvl, 1 << d, r);
+    const Node nd = lvl[i];
+    const int s = nd.lo + (r - nd.off);
+    RowOp op;
+    if (nd.rows == 1) {
+        op.h = nd.row0;
+        op.t = -1;
+        op.shift = 0;
+    } else {
+        const MergeCoef c = merge_coef(nd.rows);
+        const int h = merge_row(c.kh, s), t = merge_row(c.kt, s);
+        op.shift = (s - t) % b;
+        if (d == T.depth) {
+            op.h = nd.row0 + h;
+            op.t = nd.row0 + (nd.rows >> 1) + t;
         } else {
-            const MergeCoef c = merge_coef(nd.rows);
-            const int h = merge_row(c.kh, s), t = merge_row(c.kt, s);
-            op.shift = (s - t) % b;
-            if (d == T.depth) {
-                op.h = nd.row0 + h;
-                op.t = nd.row0 + (nd.rows >> 1) + t;
-            } else {
-                const Node hn = child[2 * i], tn = child[2 * i + 1];
-                op.h = hn.off + h - hn.lo;
-                op.t = tn.off + t - tn.lo;
-            }
+            const Node* child = T.nodes + T.level_start[d + 1];
+            const Node hn = child[2 * i], tn = child[2 * i + 1];
+            op.h = hn.off + h - hn.lo;
+            op.t = tn.off + t - tn.lo;
         }
-        ops[r] = op;
+    }
+    return op;
+}
+
+// Row operations of every level of the job (one thread per output row, all levels at once).
+// Call after build_job_tree; the caller synchronises before using `ops`.
+__device__ inline void build_all_ops(const JobTree& T, int b, RowOp* ops)
+{
+    const int total = T.op_start[T.depth + 1];
+    for (int g = threadIdx.x; g < total; g += blockDim.x) {
+        int d = 0;
+        while (T.op_start[d + 1] <= g) ++d;
+        ops[g] = make_row_op(T, d, g - T.op_start[d], b);
     }
 }
 
-// Computes the rows of one level, one warp per row. NIT = ceil(b / 32) when kUnroll.
-// kGlobal: operands are rows of the global source (packed, stride b, no halo).
+// Computes the rows of one level, one warp per row, NIT = ceil(b / 32) columns per lane.
+// kGlobal: operands are rows of the global source (packed, stride b).
 template <int NIT, bool kGlobal>
 __device__ __forceinline__ void level_rows_unrolled(const RowOp* ops, int nrows,
                                                     const float* __restrict__ src, int sstride,
@@ -216,12 +231,12 @@ __device__ __forceinline__ void level_rows_unrolled(const RowOp* ops, int nrows,
                 if (j < NIT - 1 || c < b) {
                     int base = 32 * j + op.shift;
                     base -= (base >= b) ? b : 0;
+                    int idx = base + lane;
+                    idx -= (idx >= b) ? b : 0;
                     if constexpr (kGlobal) {
-                        int idx = base + lane;
-                        idx -= (idx >= b) ? b : 0;
                         v[j] = __fadd_rn(__ldcg(H + c), __ldcg(Tr + idx));
                     } else {
-                        v[j] = __fadd_rn(H[c], Tr[base + lane]);
+                        v[j] = __fadd_rn(H[c], Tr[idx]);
                     }
                 }
             }
@@ -231,11 +246,10 @@ __device__ __forceinline__ void level_rows_unrolled(const RowOp* ops, int nrows,
             const int c = lane + 32 * j;
             if (j < NIT - 1 || c < b) out[c] = v[j];
         }
-        out[b + lane] = v[0];  // halo (b >= 32 on this path)
     }
 }
 
-// Any b: per-element wrap, no unrolling (b < 32 or b > 32 * 17).
+// Any b: per-element wrap, no unrolling.
 template <bool kGlobal>
 __device__ __forceinline__ void level_rows_generic(const RowOp* ops, int nrows,
                                                    const float* __restrict__ src, int sstride,
@@ -258,9 +272,6 @@ __device__ __forceinline__ void level_rows_generic(const RowOp* ops, int nrows,
             }
             out[c] = v;
         }
-        __syncwarp();
-        if (b >= kHalo) out[b + lane] = out[lane];
-        __syncwarp();
     }
 }
 
@@ -269,10 +280,6 @@ __device__ __forceinline__ void level_rows(const RowOp* ops, int nrows, const fl
                                            int sstride, float* dst, int stride, int b)
 {
     const int nit = (b + 31) >> 5;
-    if (b < kHalo) {
-        level_rows_generic<kGlobal>(ops, nrows, src, sstride, dst, stride, b);
-        return;
-    }
     switch (nit) {
 #define RT_NIT_CASE(N) \
     case N: level_rows_unrolled<N, kGlobal>(ops, nrows, src, sstride, dst, stride, b); break;
@@ -290,15 +297,16 @@ __device__ __forceinline__ void level_rows(const RowOp* ops, int nrows, const fl
 __device__ inline void run_job_levels(const JobTree& T, const float* __restrict__ src, int b,
                                       float* buf0, float* buf1, int stride, RowOp* ops)
 {
+    build_all_ops(T, b, ops);
+    __syncthreads();
     for (int d = T.depth; d >= 0; --d) {
         float* dst = (d & 1) ? buf1 : buf0;
         const float* prev = (d & 1) ? buf0 : buf1;  // level d+1
-        build_level_ops(T, d, b, ops);
-        __syncthreads();
+        const RowOp* lops = ops + T.op_start[d];
         if (d == T.depth)
-            level_rows<true>(ops, T.level_rows[d], src, b, dst, stride, b);
+            level_rows<true>(lops, T.level_rows[d], src, b, dst, stride, b);
         else
-            level_rows<false>(ops, T.level_rows[d], prev, stride, dst, stride, b);
+            level_rows<false>(lops, T.level_rows[d], prev, stride, dst, stride, b);
         __syncthreads();
     }
 }
@@ -309,19 +317,20 @@ __device__ __forceinline__ void store_root_rows(const JobTree& T, const float* b
 {
     const Node r = T.nodes[0];
     const int nrows = r.hi - r.lo;
-    const int total = nrows * b;
     float* base = dst + (size_t)(r.row0 + r.lo) * b;
-    for (int i = threadIdx.x; i < total; i += kThreads) {
-        const int row = i / b, c = i - row * b;
-        base[i] = buf0[(size_t)row * stride + c];
-    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int row = warp; row < nrows; row += kWarps)
+        for (int c = lane; c < b; c += 32) base[(size_t)row * b + c] = buf0[(size_t)row * stride + c];
 }
 
 // Shared-memory layout of a CTA running FFA jobs: [fixed part][ops][buf0][buf1].
 // Rows per level buffer for `smem_bytes` with `fixed_bytes` already used.
+constexpr int kOpsPerCapRow = kMaxJobDepth + 1;  // row operations of all levels of a job
+
 RT_HD int ffa_cap_rows_for(size_t smem_bytes, size_t fixed_bytes, int b)
 {
-    const size_t per_row = 2 * (size_t)ffa_stride(b) * sizeof(float) + sizeof(RowOp);
+    const size_t per_row =
+        2 * (size_t)ffa_stride(b) * sizeof(float) + kOpsPerCapRow * sizeof(RowOp);
     return (int)((smem_bytes - fixed_bytes - 64) / per_row);
 }
 
@@ -335,7 +344,7 @@ __device__ __forceinline__ FfaSmem ffa_smem(unsigned char* base, int cap_rows, i
 {
     FfaSmem L;
     L.ops = reinterpret_cast<RowOp*>(base);
-    size_t off = ((size_t)cap_rows * sizeof(RowOp) + 63) & ~size_t(63);
+    size_t off = ((size_t)cap_rows * kOpsPerCapRow * sizeof(RowOp) + 63) & ~size_t(63);
     L.buf0 = reinterpret_cast<float*>(base + off);
     L.buf1 = L.buf0 + (size_t)cap_rows * ffa_stride(b);
     return L;

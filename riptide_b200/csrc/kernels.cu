@@ -252,12 +252,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     float* C = reinterpret_cast<float*>(smem + ((sizeof(SnrParams) + 255) & ~size_t(255)));
     snr_params_fill(S, widths, nw, nfast, b);
     const int cs = prefix_stride(b, S.wmax, TPR);
+    const int groups = min(tile_rows, kThreads / TPR);
     for (int r0 = blockIdx.x * tile_rows; r0 < rows; r0 += gridDim.x * tile_rows) {
         const int nr = min(tile_rows, rows - r0);
-        prefix_rows(x + (size_t)r0 * b, b, nr, b, S.wmax, C, cs);
-        __syncthreads();
-        snr_rows_from_prefix<TPR, 17>(C, cs, nr, b, S, stdnoise, out + (size_t)r0 * nw, nw);
-        __syncthreads();
+        snr_rows<TPR, 34>(x + (size_t)r0 * b, b, nr, b, S, stdnoise, out + (size_t)r0 * nw, nw,
+                          C, cs, groups);
     }
 }
 

@@ -6,7 +6,7 @@
 namespace rt {
 
 // Dynamic shared memory of the FFA / S/N kernels (one CTA per SM).
-constexpr size_t kFfaSmemBytes = 220 * 1024;
+constexpr size_t kFfaSmemBytes = 226 * 1024;
 
 int ffa_cap_rows(int b);
 size_t ffa_scratch_floats(int m, int b);

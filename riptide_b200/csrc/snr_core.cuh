@@ -101,78 +101,139 @@ __device__ inline void prefix_rows(const float* x, int xs, int nrows, int b, int
     }
 }
 
-// Max over phases of C[i+w] - C[i] for the fast widths, register window. Each thread covers
-// phases [i0, i1) of one profile.
-template <class WS, int SB>
-__device__ __forceinline__ void window_max(const float* cr, int i0, int i1, int climit,
-                                           float (&mx)[WS::NW])
+// Double-float accumulation (Knuth's TwoSum): (hi, lo) holds a sum exactly while it needs no
+// more than about 48 significant bits -- the float32 counterpart of the reference's double
+// accumulator (kernels.hpp:75-83), which is exact up to 53 bits. round(hi + lo) is then the
+// correctly rounded prefix, i.e. the reference's float(acc). Pure FP32 adds: no conversions.
+__device__ __forceinline__ void df_add(float& hi, float& lo, float x)
 {
-    for (int base = i0; base < i1; base += SB) {
-        float win[SB + WS::WMAX];
+    const float s = __fadd_rn(hi, x);
+    const float bp = __fsub_rn(s, hi);
+    const float e = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bp)), __fsub_rn(x, bp));
+    hi = s;
+    lo = __fadd_rn(lo, e);
+}
+
+__device__ __forceinline__ void df_add2(float& hi, float& lo, float bhi, float blo)
+{
+    const float s = __fadd_rn(hi, bhi);
+    const float bp = __fsub_rn(s, hi);
+    const float e = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bp)), __fsub_rn(bhi, bp));
+    hi = s;
+    lo = __fadd_rn(__fadd_rn(lo, blo), e);
+}
+
+__device__ __forceinline__ float fmax3(float a, float b, float c)
+{
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+// Max over SB consecutive phases [start, start + SB) of C[i+w] - C[i], for the fast widths,
+// from a register window (start + SB <= b, so every phase is a real phase of the profile).
+// Threads of one profile may cover overlapping phases: a maximum does not mind duplicates.
+template <class WS, int SB>
+__device__ __forceinline__ void window_max(const float* cr, int start, float (&mx)[WS::NW])
+{
+    static_assert(SB % 2 == 0, "phase pairs");
+    float win[SB + WS::WMAX];
 #pragma unroll
-        for (int j = 0; j < SB + WS::WMAX; ++j) win[j] = cr[min(base + j, climit)];
-        const int nvalid = i1 - base;
+    for (int j = 0; j < SB + WS::WMAX; ++j) win[j] = cr[start + j];
 #pragma unroll
-        for (int j = 0; j < SB; ++j) {
-            if (j < nvalid) {
+    for (int j = 0; j < SB; j += 2) {
 #pragma unroll
-                for (int k = 0; k < WS::NW; ++k)
-                    mx[k] = fmaxf(mx[k], __fsub_rn(win[j + WS::w(k)], win[j]));
-            }
-        }
+        for (int k = 0; k < WS::NW; ++k)
+            mx[k] = fmax3(mx[k], __fsub_rn(win[j + WS::w(k)], win[j]),
+                          __fsub_rn(win[j + 1 + WS::w(k)], win[j + 1]));
     }
 }
 
-// S/N of `nrows` profiles whose prefix sums are rows of C; writes out[r * out_stride + k].
-// TPR threads per profile. `stdnoise` is the same for all rows.
+// Boxcar S/N of `nrows` folded profiles (rows of X, stride xs) straight from the FFA output:
+// TPR threads per profile build its circular prefix sum (double accumulation, group scan) in
+// the scratch rows C (stride cs), then take the width maxima from a register window. Only
+// warp-level synchronisation: a profile's TPR threads are lanes of one warp. Writes
+// out[r * out_stride + k]. `groups` profiles are processed at a time (C holds `groups` rows).
 template <int TPR, int SB>
-__device__ void snr_rows_from_prefix(const float* C, int cs, int nrows, int b, const SnrParams& S,
-                                     float stdnoise, float* __restrict__ out, size_t out_stride)
+__device__ void snr_rows(const float* X, int xs, int nrows, int b, const SnrParams& S,
+                         float stdnoise, float* __restrict__ out, size_t out_stride, float* C,
+                         int cs, int groups)
 {
     const int tid = threadIdx.x;
-    const int rows_per_pass = blockDim.x / TPR;
     const int g = tid / TPR, t = tid - g * TPR;
+    const int ngroups = min(groups, (int)(blockDim.x / TPR));
     const int P = ((b + TPR - 1) / TPR) | 1;  // odd: threads of a profile hit distinct banks
     const int i0 = min(b, t * P), i1 = min(b, i0 + P);
-    const int climit = b + S.wmax - 1;
-    for (int r0 = 0; r0 < nrows; r0 += rows_per_pass) {
-        const int r = r0 + g;
-        const bool active = r < nrows;  // whole TPR groups share `active`
-        const float* cr = C + (size_t)(active ? r : 0) * cs;
+    const unsigned gmask = (TPR == 32) ? 0xffffffffu : (((1u << TPR) - 1u) << ((tid & 31) & ~(TPR - 1)));
+    if (g >= ngroups) return;  // whole groups leave together
+    float* cr = C + (size_t)g * cs;
+    for (int r = g; r < nrows; r += ngroups) {
+        const float* xr = X + (size_t)r * xs;
+        // prefix sums (kernels.hpp:73-101): exact sums (double-float), float stores
+        float lh = 0.f, ll = 0.f;
+        for (int i = i0; i < i1; ++i) df_add(lh, ll, xr[i]);
+        float ih = lh, il = ll;  // inclusive scan over the TPR segments
+#pragma unroll
+        for (int o = 1; o < TPR; o <<= 1) {
+            const float yh = __shfl_up_sync(gmask, ih, o, TPR);
+            const float yl = __shfl_up_sync(gmask, il, o, TPR);
+            if (t >= o) {
+                // (earlier segments) + (this range), in order of increasing phase
+                float nh = yh, nl = yl;
+                df_add2(nh, nl, ih, il);
+                ih = nh;
+                il = nl;
+            }
+        }
+        float rh = __shfl_up_sync(gmask, ih, 1, TPR), rl = __shfl_up_sync(gmask, il, 1, TPR);
+        if (t == 0) rh = rl = 0.f;
+        for (int i = i0; i < i1; ++i) {
+            df_add(rh, rl, xr[i]);
+            cr[i] = __fadd_rn(rh, rl);
+        }
+        const float th = __shfl_sync(gmask, ih, TPR - 1, TPR), tl = __shfl_sync(gmask, il, TPR - 1, TPR);
+        const float sumx = __fadd_rn(th, tl);
+        __syncwarp(gmask);
+        for (int j = t; j < S.wmax; j += TPR) cr[b + j] = __fadd_rn(cr[j], sumx);
+        __syncwarp(gmask);
+        const float sum = cr[b - 1];
         float mx[FastWidths10::NW];
 #pragma unroll
         for (int k = 0; k < FastWidths10::NW; ++k) mx[k] = -INFINITY;
-        if (active && S.nfast == FastWidths10::NW)
-            window_max<FastWidths10, SB>(cr, i0, i1, climit, mx);
+        if (S.nfast == FastWidths10::NW) {
+            if (b >= SB && P <= SB) {
+                window_max<FastWidths10, SB>(cr, min(i0, b - SB), mx);
+            } else {
+                for (int i = i0; i < i1; ++i)
+#pragma unroll
+                    for (int k = 0; k < FastWidths10::NW; ++k)
+                        mx[k] = fmaxf(mx[k], __fsub_rn(cr[i + FastWidths10::w(k)], cr[i]));
+            }
+        }
 #pragma unroll
         for (int k = 0; k < FastWidths10::NW; ++k) {
 #pragma unroll
             for (int o = TPR / 2; o > 0; o >>= 1)
-                mx[k] = fmaxf(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+                mx[k] = fmaxf(mx[k], __shfl_xor_sync(gmask, mx[k], o, TPR));
         }
-        const float sum = active ? cr[b - 1] : 0.f;
-        if (active) {
-            float* orow = out + (size_t)r * out_stride;
-            for (int k = t; k < S.nfast; k += TPR) {
-                float dm = mx[0];
+        float* orow = out + (size_t)r * out_stride;
+        for (int k = t; k < S.nfast; k += TPR) {
+            float dm = mx[0];
 #pragma unroll
-                for (int q = 1; q < FastWidths10::NW; ++q) dm = (k == q) ? mx[q] : dm;
-                orow[k] = __fdiv_rn(__fmaf_rn(S.hb[k], dm, -__fmul_rn(S.beta[k], sum)), stdnoise);
-            }
+            for (int q = 1; q < FastWidths10::NW; ++q) dm = (k == q) ? mx[q] : dm;
+            orow[k] = __fdiv_rn(__fmaf_rn(S.hb[k], dm, -__fmul_rn(S.beta[k], sum)), stdnoise);
         }
-        // remaining widths: direct shared-memory reads, one width per pass
+        // remaining widths: direct shared-memory reads
         for (int k = S.nfast; k < S.nw; ++k) {
             const int w = S.w[k];
             float m = -INFINITY;
-            if (active)
-                for (int i = i0; i < i1; ++i) m = fmaxf(m, __fsub_rn(cr[i + w], cr[i]));
+            for (int i = i0; i < i1; ++i) m = fmaxf(m, __fsub_rn(cr[i + w], cr[i]));
 #pragma unroll
-            for (int o = TPR / 2; o > 0; o >>= 1)
-                m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-            if (active && t == 0)
-                out[(size_t)r * out_stride + k] =
-                    __fdiv_rn(__fmaf_rn(S.hb[k], m, -__fmul_rn(S.beta[k], sum)), stdnoise);
+            for (int o = TPR / 2; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(gmask, m, o, TPR));
+            if (t == 0)
+                orow[k] = __fdiv_rn(__fmaf_rn(S.hb[k], m, -__fmul_rn(S.beta[k], sum)), stdnoise);
         }
+        __syncwarp(gmask);  // cr is rewritten for the next profile
     }
 }
 
