@@ -61,13 +61,15 @@ def _pulse(torch, n, period_samples, ducy, amplitude, phi0, device):
 
 
 def _red(torch, n, rms, gen, device):
-    w = torch.randn(n, generator=gen, device=device, dtype=torch.float32)
+    # shaped on the next power-of-two length (one FFT size for every trial), then cut to n
+    nf = 1 << max(0, (n - 1).bit_length())
+    w = torch.randn(nf, generator=gen, device=device, dtype=torch.float32)
     X = torch.fft.rfft(w)
     f = torch.arange(X.numel(), device=device, dtype=torch.float32)
     f[0] = 1.0
     X = X / torch.sqrt(f)
     X[0] = 0
-    r = torch.fft.irfft(X, n=n)
+    r = torch.fft.irfft(X, n=nf)[:n]
     return r * (rms / r.std())
 
 
