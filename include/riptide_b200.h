@@ -57,6 +57,15 @@ int rt_circular_prefix_sum(const float* d_x, size_t size, size_t nsum, float* d_
  * blocks larger than one CTA's shared memory. */
 int rt_ffa2(const float* d_in, size_t rows, size_t cols, float* d_out, void* stream);
 
+/* ffa2 without any device allocation, for callers that cannot allocate: pipelines whose
+ * device memory is reserved up front by another framework's pool, and real-time loops that
+ * forbid cudaMalloc/cudaFree after start-up (they can block the whole device). No counterpart
+ * in the reference. Scratch is a fixed 8 MiB array in this library, held by every GPU that
+ * loads it: rows * cols <= 1048576 (cols <= 4096), else RT_EINVAL. The first call on a device
+ * looks the array up (cudaGetSymbolAddress) and should come before any stream capture. Calls
+ * share the array: calls that overlap on the GPU race and must not be issued. */
+int rt_ffa2_noalloc(const float* d_in, size_t rows, size_t cols, float* d_out, void* stream);
+
 /* benchmark_ffa2: seconds per transform of a zero rows x cols block over `loops` runs
  * (CUDA events). Replaces python_bindings.cpp:99-118. */
 int rt_benchmark_ffa2(size_t rows, size_t cols, size_t loops, double* h_seconds);

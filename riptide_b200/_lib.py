@@ -28,6 +28,7 @@ SIGNATURES = {
     "rt_fused_rollback_add": (ctypes.c_int, [_vp, _vp, _sz, _sz, _vp, _vp]),
     "rt_circular_prefix_sum": (ctypes.c_int, [_vp, _sz, _sz, _vp, _vp]),
     "rt_ffa2": (ctypes.c_int, [_vp, _sz, _sz, _vp, _vp]),
+    "rt_ffa2_noalloc": (ctypes.c_int, [_vp, _sz, _sz, _vp, _vp]),
     "rt_benchmark_ffa2": (ctypes.c_int, [_sz, _sz, _sz, ctypes.POINTER(_d)]),
     "rt_snr2": (ctypes.c_int, [_vp, _sz, _sz, _u64p, _sz, ctypes.c_float, _vp, _vp]),
     "rt_downsample": (ctypes.c_int, [_vp, _sz, _d, _vp, _vp]),
