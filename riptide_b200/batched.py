@@ -134,7 +134,7 @@ class BatchedSearch(object):
         c = np.zeros(8, dtype=np.uint64)
         _lib.check(_lib.load().rt_search_phase_cycles(self._plan, c.ctypes.data_as(_lib._u64p),
                                                       int(bool(reset))))
-        names = ["fetch", "wait", "tree", "levels", "snr", "store"]
+        names = ["fetch", "wait", "tree", "levels", "snr", "store", "decode"]
         return {n: int(c[i]) for i, n in enumerate(names)}
 
     def close(self):

@@ -115,23 +115,98 @@ __device__ void final_stage_outputs(const JobTree& T, const XformRec& X, const E
                       A.snrs + ((size_t)X.out_row + r.lo) * S.nw, S.nw, buf1, cs, groups);
     double* per_out = A.periods + X.out_row;
     uint32_t* fb_out = A.foldbins + X.out_row;
-    for (int s = r.lo + threadIdx.x; s < r.hi; s += blockDim.x) {
+    for (int s = r.lo + threadIdx.x; s < r.hi; s += kThreads) {
         per_out[s] = trial_period(X.tau, b, s, X.m);
         fb_out[s] = (uint32_t)b;
     }
 }
 
-__global__ void __launch_bounds__(kThreads, 1) k_search_persistent(EngineArgs A)
+// The persistent kernel has kThreads compute threads and one scheduling warp. The scheduler
+// claims the next ticket, loads its descriptors into one of two shared slots and waits for
+// its dependencies while the compute threads work on the other slot; slot hand-over uses
+// named barriers (full: scheduler -> compute, empty: compute -> scheduler), one pair per slot.
+constexpr int kEngineThreads = kThreads + 32;
+constexpr int kBarFull = 2;   // + slot
+constexpr int kBarEmpty = 4;  // + slot
+
+struct ItemSlot {
+    long long ticket;   // >= nitems: no more work
+    int ok;             // 0: a wait failed, stop
+    int stage, last, cap_rows, jobs_of_stage;
+    JobSpec J;
+    XformRec X;
+};
+
+__device__ __forceinline__ void named_sync(int id, int n)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+__device__ __forceinline__ void named_arrive(int id, int n)
+{
+    asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+
+__device__ void scheduler_warp(const EngineArgs& A, ItemSlot* slots)
+{
+    const int lane = threadIdx.x & 31;
+    int k = 0;
+    for (;; ++k) {
+        const int s = k & 1;
+        if (k >= 2) named_sync(kBarEmpty + s, kEngineThreads);  // compute is done with item k-2
+        if (lane == 0) {
+            ItemSlot& L = slots[s];
+            const long long t = (ld_acquire(A.error) != RT_OK)
+                                    ? A.nitems
+                                    : (long long)atomicAdd(A.ticket, 1ull);
+            L.ticket = t;
+            L.ok = 1;
+            if (t < A.nitems) {
+                const WorkItem W = A.items[t];
+                const XformRec X = A.xforms[W.xform];
+                const StagePlan P = A.plans[X.plan];
+                const int stage = W.stage_job >> 24, job = W.stage_job & 0xffffff;
+                const JobSpec J = stage_job(X.m, X.rows_eval, P, stage, job);
+                L.X = X;
+                L.J = J;
+                L.stage = stage;
+                L.last = stage == P.nstages - 1;
+                L.jobs_of_stage = P.jobs[stage];
+                L.cap_rows = engine_cap_rows(X.b);
+                if (J.hi > J.lo && X.seq >= 0) {
+                    const int seq = X.seq;
+                    bool ok;
+                    if (stage == 0)
+                        ok = wait_at_least(A.slot_release + (seq % kSlots), seq / kSlots, A.error);
+                    else
+                        ok = wait_at_least(A.done + (size_t)seq * kMaxStages + stage - 1,
+                                           P.jobs[stage - 1], A.error);
+                    L.ok = ok ? 1 : 0;
+                }
+            }
+            __threadfence_block();
+        }
+        __syncwarp();
+        const bool stop = slots[s].ticket >= A.nitems || !slots[s].ok;
+        named_arrive(kBarFull + s, kEngineThreads);
+        if (stop) break;
+    }
+    // the compute threads still hand back the slot of item k-1
+    if (k >= 1) named_sync(kBarEmpty + ((k - 1) & 1), kEngineThreads);
+}
+
+__global__ void __launch_bounds__(kEngineThreads, 1) k_search_persistent(EngineArgs A)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     JobTree& T = *reinterpret_cast<JobTree*>(smem);
     SnrParams& S = *reinterpret_cast<SnrParams*>(smem + kEngineTreeBytes);
     unsigned char* layout = smem + kEngineTreeBytes + kEngineSnrBytes;
-    __shared__ long long s_item;
-    __shared__ int s_ok;
+    __shared__ ItemSlot slots[2];
     __shared__ int s_b;
-    if (threadIdx.x == 0) s_b = -1;
 
+    if (threadIdx.x >= kThreads) {
+        scheduler_warp(A, slots);
+        return;
+    }
     const bool prof = A.phase_cycles != nullptr;
     unsigned long long ph[kPhases] = {0, 0, 0, 0, 0, 0, 0, 0};
     long long tprev = prof ? clock64() : 0;
@@ -142,83 +217,68 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_persistent(EngineArgs A)
             tprev = t;
         }
     };
-    for (;;) {
-        if (threadIdx.x == 0) {
-            s_item = (ld_acquire(A.error) != RT_OK) ? A.nitems
-                                                    : (long long)atomicAdd(A.ticket, 1ull);
-        }
-        __syncthreads();
-        const long long it = s_item;
-        if (it >= A.nitems) break;
-        const WorkItem W = A.items[it];
-        const XformRec X = A.xforms[W.xform];
-        const StagePlan& P = A.plans[X.plan];
-        const int stage = W.stage_job >> 24, job = W.stage_job & 0xffffff;
-        const bool last = stage == P.nstages - 1;
-        const JobSpec J = stage_job(X.m, X.rows_eval, P, stage, job);
+    if (threadIdx.x == 0) s_b = -1;
+    for (int k = 0;; ++k) {
+        const int sl = k & 1;
+        named_sync(kBarFull + sl, kEngineThreads);
+        mark(kPhWait);
+        const ItemSlot& L = slots[sl];
+        if (L.ticket >= A.nitems || !L.ok) break;
+        const XformRec X = L.X;
+        const JobSpec J = L.J;
+        const int stage = L.stage;
+        const bool last = L.last != 0;
+        const int jobs_of_stage = L.jobs_of_stage;
         const int b = X.b;
         const int fstride = ffa_stride(b);
-        const int cap_rows = engine_cap_rows(b);
-        const FfaSmem L = ffa_smem(layout, cap_rows, b);
-        float* buf0 = L.buf0;
-        float* buf1 = L.buf1;
+        const int cap_rows = L.cap_rows;
+        const FfaSmem Lay = ffa_smem(layout, cap_rows, b);
         float* slot = (X.seq >= 0) ? A.scratch + (size_t)(X.seq % kSlots) * 2 * A.slot_floats
                                    : nullptr;
-        mark(kPhFetch);
-        if (threadIdx.x == 0) {
-            s_ok = 1;
-            if (J.hi > J.lo && X.seq >= 0) {
-                bool ok;
-                if (stage == 0)
-                    ok = wait_at_least(A.slot_release + (X.seq % kSlots), X.seq / kSlots, A.error);
-                else
-                    ok = wait_at_least(A.done + (size_t)X.seq * kMaxStages + stage - 1,
-                                       P.jobs[stage - 1], A.error);
-                s_ok = ok ? 1 : 0;
-            }
-        }
-        if (b != s_b) {
-            // boxcar coefficients depend on b
-            __syncthreads();
+        mark(6);
+        if (b != s_b) {  // boxcar coefficients depend on b
             snr_params_fill(S, A.widths, A.nw, A.nfast, b);
             if (threadIdx.x == 0) s_b = b;
+            cta_sync();
         }
-        __syncthreads();
-        mark(kPhWait);
-        if (!s_ok) break;
+        mark(kPhFetch);
+        bool failed = false;
         if (J.hi > J.lo) {
             const float* src =
                 (stage == 0) ? (X.src_norm ? A.norm : A.ds) + X.src_off
                              : slot + (size_t)((stage - 1) & 1) * A.slot_floats;
             build_job_tree(T, J, cap_rows);
-            if (T.error) {
+            failed = T.error != 0;
+            if (failed) {
                 if (threadIdx.x == 0) atomicExch(A.error, RT_EINTERNAL);
-                break;
-            }
-            mark(kPhTree);
-            run_job_levels(T, src, b, buf0, buf1, fstride, L.ops);
-            mark(kPhLevels);
-            if (last) {
-                if (snr_tpr(b) == 8)
-                    final_stage_outputs<8>(T, X, A, S, buf0, buf1, fstride, cap_rows);
-                else
-                    final_stage_outputs<16>(T, X, A, S, buf0, buf1, fstride, cap_rows);
-                mark(kPhSnr);
             } else {
-                store_root_rows(T, buf0, fstride, b, slot + (size_t)(stage & 1) * A.slot_floats);
+                mark(kPhTree);
+                run_job_levels(T, src, b, Lay.buf0, Lay.buf1, fstride, Lay.ops);
+                mark(kPhLevels);
+                if (last) {
+                    if (snr_tpr(b) == 8)
+                        final_stage_outputs<8>(T, X, A, S, Lay.buf0, Lay.buf1, fstride, cap_rows);
+                    else
+                        final_stage_outputs<16>(T, X, A, S, Lay.buf0, Lay.buf1, fstride, cap_rows);
+                    mark(kPhSnr);
+                } else {
+                    store_root_rows(T, Lay.buf0, fstride, b,
+                                    slot + (size_t)(stage & 1) * A.slot_floats);
+                }
             }
         }
-        __syncthreads();
-        if (threadIdx.x == 0 && X.seq >= 0) {
+        cta_sync();
+        if (threadIdx.x == 0 && X.seq >= 0 && !failed) {
             __threadfence();
             int* d = A.done + (size_t)X.seq * kMaxStages + stage;
             const int prev = atomicAdd(d, 1);
-            if (last && prev + 1 == P.jobs[stage]) {
+            if (last && prev + 1 == jobs_of_stage) {
                 __threadfence();
                 atomicAdd(A.slot_release + (X.seq % kSlots), 1);
             }
         }
         mark(kPhStore);
+        named_arrive(kBarEmpty + sl, kEngineThreads);
     }
     if (prof && threadIdx.x == 0)
         for (int i = 0; i < kPhases; ++i) atomicAdd(A.phase_cycles + i, ph[i]);
@@ -737,7 +797,7 @@ static int engine_grid()
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_search_persistent, kThreads,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_search_persistent, kEngineThreads,
                                                   kFfaSmemBytes);
     return std::max(1, sms * std::max(per, 1));
 }
@@ -846,7 +906,7 @@ static int plan_run(SearchPlan& P, const float* data, float* normalised_out, dou
                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)kFfaSmemBytes));
     if (A.nitems > 0) {
-        k_search_persistent<<<engine_grid(), kThreads, kFfaSmemBytes, st>>>(A);
+        k_search_persistent<<<engine_grid(), kEngineThreads, kFfaSmemBytes, st>>>(A);
         RT_TRY_CUDA(cudaGetLastError());
         launches += 1;
     }

@@ -24,8 +24,15 @@ namespace rt {
 
 constexpr int kMaxJobDepth = 7;      // levels computed inside one job (<= 128 nodes at the bottom)
 constexpr int kMaxJobNodes = 256;    // total nodes of all levels of one job
-constexpr int kThreads = 512;        // threads per CTA of every FFA kernel (1 CTA per SM)
+constexpr int kThreads = 480;        // compute threads per CTA of every FFA kernel (1 CTA per SM)
 constexpr int kWarps = kThreads / 32;
+
+// Barrier of the compute threads only (named barrier 1). The persistent search kernel adds a
+// scheduling warp that does not take part; in the other kernels every thread computes.
+__device__ __forceinline__ void cta_sync()
+{
+    asm volatile("bar.sync 1, %0;" ::"n"(kThreads) : "memory");
+}
 
 struct Node {
     int row0;   // first row of the node in the transform
@@ -73,11 +80,11 @@ __device__ inline void build_job_tree(JobTree& T, const JobSpec& J, int cap_rows
         T.error = bad ? 1 : 0;
     }
     if (bad) {
-        __syncthreads();
+        cta_sync();
         return;
     }
     const int nnodes = (2 << G) - 1;
-    for (int q = tid; q < nnodes; q += blockDim.x) {
+    for (int q = tid; q < nnodes; q += kThreads) {
         const int d = 31 - __clz(q + 1);
         const int i = q + 1 - (1 << d);
         int row0 = J.root_row0, rows = J.root_rows, lo = J.lo, hi = J.hi;
@@ -106,7 +113,7 @@ __device__ inline void build_job_tree(JobTree& T, const JobSpec& J, int cap_rows
         T.nodes[q] = nd;
     }
     if (tid <= G) T.level_start[tid] = (1 << tid) - 1;
-    __syncthreads();
+    cta_sync();
     // one warp per level: exclusive prefix of the row counts -> buffer offsets
     const int warp = tid >> 5, lane = tid & 31;
     if (warp <= G) {
@@ -129,7 +136,7 @@ __device__ inline void build_job_tree(JobTree& T, const JobSpec& J, int cap_rows
             if (carry > cap_rows) T.error = 2;
         }
     }
-    __syncthreads();
+    cta_sync();
     if (tid == 0) {
         int acc = 0;
         for (int d = 0; d <= G; ++d) {
@@ -138,7 +145,7 @@ __device__ inline void build_job_tree(JobTree& T, const JobSpec& J, int cap_rows
         }
         T.op_start[G + 1] = acc;
     }
-    __syncthreads();
+    cta_sync();
 }
 
 // Index of the node holding buffer row r at a level (nodes sorted by `off`).
@@ -197,7 +204,7 @@ __device__ __forceinline__ RowOp make_row_op(const JobTree& T, int d, int r, int
 __device__ inline void build_all_ops(const JobTree& T, int b, RowOp* ops)
 {
     const int total = T.op_start[T.depth + 1];
-    for (int g = threadIdx.x; g < total; g += blockDim.x) {
+    for (int g = threadIdx.x; g < total; g += kThreads) {
         int d = 0;
         while (T.op_start[d + 1] <= g) ++d;
         ops[g] = make_row_op(T, d, g - T.op_start[d], b);
@@ -229,15 +236,11 @@ __device__ __forceinline__ void level_rows_unrolled(const RowOp* ops, int nrows,
             for (int j = 0; j < NIT; ++j) {
                 const int c = lane + 32 * j;
                 if (j < NIT - 1 || c < b) {
-                    int base = 32 * j + op.shift;
-                    base -= (base >= b) ? b : 0;
-                    int idx = base + lane;
+                    int p0 = 32 * j + op.shift;
+                    p0 -= (p0 >= b) ? b : 0;
+                    int idx = p0 + lane;
                     idx -= (idx >= b) ? b : 0;
-                    if constexpr (kGlobal) {
-                        v[j] = __fadd_rn(__ldcg(H + c), __ldcg(Tr + idx));
-                    } else {
-                        v[j] = __fadd_rn(H[c], Tr[idx]);
-                    }
+                    v[j] = __fadd_rn(kGlobal ? __ldcg(H + c) : H[c], kGlobal ? __ldcg(Tr + idx) : Tr[idx]);
                 }
             }
         }
@@ -298,7 +301,7 @@ __device__ inline void run_job_levels(const JobTree& T, const float* __restrict_
                                       float* buf0, float* buf1, int stride, RowOp* ops)
 {
     build_all_ops(T, b, ops);
-    __syncthreads();
+    cta_sync();
     for (int d = T.depth; d >= 0; --d) {
         float* dst = (d & 1) ? buf1 : buf0;
         const float* prev = (d & 1) ? buf0 : buf1;  // level d+1
@@ -307,7 +310,7 @@ __device__ inline void run_job_levels(const JobTree& T, const float* __restrict_
             level_rows<true>(lops, T.level_rows[d], src, b, dst, stride, b);
         else
             level_rows<false>(lops, T.level_rows[d], prev, stride, dst, stride, b);
-        __syncthreads();
+        cta_sync();
     }
 }
 

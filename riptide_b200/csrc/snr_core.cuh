@@ -15,6 +15,7 @@
 // holding a window C[i .. i+SB+WMAX) in registers so that every width reads registers only.
 #pragma once
 #include "common.cuh"
+#include "ffa_core.cuh"
 
 namespace rt {
 
@@ -60,45 +61,11 @@ __device__ inline void snr_params_fill(SnrParams& S, const int* widths, int nw, 
         for (int k = 0; k < nw; ++k) wm = widths[k] > wm ? widths[k] : wm;
         S.wmax = wm;
     }
-    for (int k = threadIdx.x; k < nw; k += blockDim.x) {
+    for (int k = threadIdx.x; k < nw; k += kThreads) {
         S.w[k] = widths[k];
         boxcar_coefs(b, widths[k], &S.hb[k], &S.beta[k]);
     }
-    __syncthreads();
-}
-
-// Circular prefix sums of `nrows` profiles (rows of `x`, stride xs) into C (stride cs, each row
-// b + wmax entries). One warp per profile.
-__device__ inline void prefix_rows(const float* x, int xs, int nrows, int b, int wmax, float* C, int cs)
-{
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nw_ = blockDim.x >> 5;
-    const int K = ((b + 31) >> 5) | 1;  // odd chunk: the 32 lanes hit distinct banks
-    for (int r = warp; r < nrows; r += nw_) {
-        const float* xr = x + (size_t)r * xs;
-        float* cr = C + (size_t)r * cs;
-        const int c0 = lane * K;
-        const int c1 = min(b, c0 + K);
-        double local = 0.0;
-        for (int c = c0; c < c1; ++c) local += (double)xr[c];
-        double incl = local;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const double y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        double run = __shfl_up_sync(0xffffffffu, incl, 1);
-        if (lane == 0) run = 0.0;
-        for (int c = c0; c < c1; ++c) {
-            run += (double)xr[c];
-            cr[c] = __double2float_rn(run);
-        }
-        const double total = __shfl_sync(0xffffffffu, incl, 31);
-        const float sumx = __double2float_rn(total);
-        __syncwarp();
-        for (int j = lane; j < wmax; j += 32) cr[b + j] = __fadd_rn(cr[j], sumx);
-        __syncwarp();
-    }
+    cta_sync();
 }
 
 // Double-float accumulation (Knuth's TwoSum): (hi, lo) holds a sum exactly while it needs no
@@ -161,7 +128,7 @@ __device__ void snr_rows(const float* X, int xs, int nrows, int b, const SnrPara
 {
     const int tid = threadIdx.x;
     const int g = tid / TPR, t = tid - g * TPR;
-    const int ngroups = min(groups, (int)(blockDim.x / TPR));
+    const int ngroups = min(groups, kThreads / TPR);
     const int P = ((b + TPR - 1) / TPR) | 1;  // odd: threads of a profile hit distinct banks
     const int i0 = min(b, t * P), i1 = min(b, i0 + P);
     const unsigned gmask = (TPR == 32) ? 0xffffffffu : (((1u << TPR) - 1u) << ((tid & 31) & ~(TPR - 1)));
