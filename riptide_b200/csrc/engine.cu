@@ -52,7 +52,7 @@ RT_HD int engine_cap_rows(int b)
     return ffa_cap_rows_for(kFfaSmemBytes, kEngineTreeBytes + kEngineSnrBytes, b);
 }
 
-constexpr int kSlots = 48;           // scratch slots for multi-stage transforms
+constexpr int kSlots = 256;          // scratch slots for multi-stage transforms
 constexpr size_t kLagItems = 640;    // work items emitted between two stages of a transform
 constexpr long long kSpinLimit = 20000000LL;  // bounded waits (about 2-20 s with backoff)
 
@@ -79,6 +79,9 @@ struct EngineArgs {
 
 // Phases of one work item, for the optional in-kernel profile.
 enum { kPhFetch = 0, kPhWait, kPhTree, kPhLevels, kPhSnr, kPhStore, kPhases = 8 };
+// extra counters after the phases: blocked on a scratch slot, blocked on a previous stage,
+// items claimed, scheduler polls that found nothing ready
+constexpr int kCounters = 12;
 
 __device__ __forceinline__ int ld_acquire(const int* p)
 {
@@ -146,43 +149,117 @@ __device__ __forceinline__ void named_arrive(int id, int n)
     asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(n) : "memory");
 }
 
+// Scheduler-side view of a claimed item: its slot contents and its dependency.
+struct SchedItem {
+    ItemSlot slot;
+    const int* dep;     // counter to wait for (null: no dependency)
+    int target;         // ... until it reaches this value
+};
+
+__device__ __forceinline__ bool sched_ready(const SchedItem& it)
+{
+    return it.dep == nullptr || ld_acquire(it.dep) >= it.target;
+}
+
+__device__ void sched_decode(const EngineArgs& A, long long t, SchedItem& it)
+{
+    ItemSlot& L = it.slot;
+    const WorkItem W = A.items[t];
+    const XformRec X = A.xforms[W.xform];
+    const StagePlan P = A.plans[X.plan];
+    const int stage = W.stage_job >> 24, job = W.stage_job & 0xffffff;
+    const JobSpec J = stage_job(X.m, X.rows_eval, P, stage, job);
+    L.ticket = t;
+    L.ok = 1;
+    L.X = X;
+    L.J = J;
+    L.stage = stage;
+    L.last = stage == P.nstages - 1;
+    L.jobs_of_stage = P.jobs[stage];
+    L.cap_rows = engine_cap_rows(X.b);
+    it.dep = nullptr;
+    it.target = 0;
+    if (J.hi > J.lo && X.seq >= 0) {
+        const int seq = X.seq;
+        if (stage == 0) {
+            it.dep = A.slot_release + (seq % kSlots);
+            it.target = seq / kSlots;
+        } else {
+            it.dep = A.done + (size_t)seq * kMaxStages + stage - 1;
+            it.target = P.jobs[stage - 1];
+        }
+    }
+}
+
+// Hands the compute threads one ready item per slot. Items whose dependency is not met yet
+// are parked (up to kParked) while later tickets are tried, so a waiting stage does not stall
+// the CTA. Progress: the smallest unfinished ticket has all its dependencies finished (they
+// have smaller tickets), so whichever scheduler holds it hands it over; every wait is bounded.
+constexpr int kParked = 4;
+
 __device__ void scheduler_warp(const EngineArgs& A, ItemSlot* slots)
 {
     const int lane = threadIdx.x & 31;
+    SchedItem parked[kParked];
+    int nparked = 0;
+    bool exhausted = false;
     int k = 0;
     for (;; ++k) {
         const int s = k & 1;
         if (k >= 2) named_sync(kBarEmpty + s, kEngineThreads);  // compute is done with item k-2
         if (lane == 0) {
             ItemSlot& L = slots[s];
-            const long long t = (ld_acquire(A.error) != RT_OK)
-                                    ? A.nitems
-                                    : (long long)atomicAdd(A.ticket, 1ull);
-            L.ticket = t;
-            L.ok = 1;
-            if (t < A.nitems) {
-                const WorkItem W = A.items[t];
-                const XformRec X = A.xforms[W.xform];
-                const StagePlan P = A.plans[X.plan];
-                const int stage = W.stage_job >> 24, job = W.stage_job & 0xffffff;
-                const JobSpec J = stage_job(X.m, X.rows_eval, P, stage, job);
-                L.X = X;
-                L.J = J;
-                L.stage = stage;
-                L.last = stage == P.nstages - 1;
-                L.jobs_of_stage = P.jobs[stage];
-                L.cap_rows = engine_cap_rows(X.b);
-                if (J.hi > J.lo && X.seq >= 0) {
-                    const int seq = X.seq;
-                    bool ok;
-                    if (stage == 0)
-                        ok = wait_at_least(A.slot_release + (seq % kSlots), seq / kSlots, A.error);
-                    else
-                        ok = wait_at_least(A.done + (size_t)seq * kMaxStages + stage - 1,
-                                           P.jobs[stage - 1], A.error);
-                    L.ok = ok ? 1 : 0;
+            const long long w0 = clock64();
+            bool chosen = false;
+            unsigned ns = 32;
+            for (long long spin = 0; !chosen; ++spin) {
+                for (int i = 0; i < nparked && !chosen; ++i) {
+                    if (sched_ready(parked[i])) {
+                        L = parked[i].slot;
+                        for (int q = i; q + 1 < nparked; ++q) parked[q] = parked[q + 1];
+                        --nparked;
+                        chosen = true;
+                    }
                 }
+                if (chosen) break;
+                if (ld_acquire(A.error) != RT_OK) exhausted = true;
+                if (!exhausted && nparked < kParked) {
+                    const long long t = (long long)atomicAdd(A.ticket, 1ull);
+                    if (t >= A.nitems) {
+                        exhausted = true;
+                    } else {
+                        SchedItem it;
+                        sched_decode(A, t, it);
+                        if (A.phase_cycles) atomicAdd(A.phase_cycles + 10, 1ull);
+                        if (sched_ready(it)) {
+                            L = it.slot;
+                            chosen = true;
+                        } else {
+                            if (A.phase_cycles)
+                                atomicAdd(A.phase_cycles + (it.slot.stage == 0 ? 8 : 9), 1ull);
+                            parked[nparked++] = it;
+                        }
+                    }
+                    continue;
+                }
+                if (exhausted && (nparked == 0 || ld_acquire(A.error) != RT_OK)) {
+                    L.ticket = A.nitems;  // no more work
+                    L.ok = 1;
+                    chosen = true;
+                    break;
+                }
+                if (spin > kSpinLimit) {
+                    atomicExch(A.error, RT_ETIMEOUT);
+                    L.ticket = A.nitems;
+                    L.ok = 0;
+                    chosen = true;
+                    break;
+                }
+                if (A.phase_cycles) atomicAdd(A.phase_cycles + 11, 1ull);
+                __nanosleep(ns);
+                if (ns < 1024) ns <<= 1;
             }
+            if (A.phase_cycles) atomicAdd(A.phase_cycles + 7, (unsigned long long)(clock64() - w0));
             __threadfence_block();
         }
         __syncwarp();
@@ -202,11 +279,15 @@ __global__ void __launch_bounds__(kEngineThreads, 1) k_search_persistent(EngineA
     unsigned char* layout = smem + kEngineTreeBytes + kEngineSnrBytes;
     __shared__ ItemSlot slots[2];
     __shared__ int s_b;
+    __shared__ __align__(8) uint64_t s_bar;  // completion of the bulk copy of a job's rows
 
+    if (threadIdx.x == 0) mbar_init(&s_bar, 1);
+    __syncthreads();
     if (threadIdx.x >= kThreads) {
         scheduler_warp(A, slots);
         return;
     }
+    uint32_t bar_phase = 0;
     const bool prof = A.phase_cycles != nullptr;
     unsigned long long ph[kPhases] = {0, 0, 0, 0, 0, 0, 0, 0};
     long long tprev = prof ? clock64() : 0;
@@ -247,13 +328,35 @@ __global__ void __launch_bounds__(kEngineThreads, 1) k_search_persistent(EngineA
             const float* src =
                 (stage == 0) ? (X.src_norm ? A.norm : A.ds) + X.src_off
                              : slot + (size_t)((stage - 1) & 1) * A.slot_floats;
+            // stage-0 jobs (whole subtrees) read one contiguous block of rows of the
+            // downsampled arena (padded): copy it into the buffer level G reads from, in the
+            // background of the job-tree build
+            const bool staged = stage == 0 && !X.src_norm && J.root_rows <= cap_rows &&
+                                (size_t)J.root_rows * b + 8 <= (size_t)cap_rows * fstride;
+            const float* staged_src = nullptr;
+            if (staged) {
+                float* sbuf = (J.G & 1) ? Lay.buf0 : Lay.buf1;
+                __shared__ int s_delta;
+                if (threadIdx.x == 0)
+                    s_delta = stage_rows_async(sbuf, src + (size_t)J.root_row0 * b,
+                                               (size_t)J.root_rows * b, &s_bar);
+                cta_sync();
+                staged_src = sbuf + s_delta - (ptrdiff_t)J.root_row0 * b;
+            }
             build_job_tree(T, J, cap_rows);
             failed = T.error != 0;
             if (failed) {
                 if (threadIdx.x == 0) atomicExch(A.error, RT_EINTERNAL);
+                if (staged) {  // still let the copy land before the buffer is reused
+                    mbar_wait(&s_bar, bar_phase);
+                    bar_phase ^= 1u;
+                }
             } else {
                 mark(kPhTree);
-                run_job_levels(T, src, b, Lay.buf0, Lay.buf1, fstride, Lay.ops);
+                if (!run_job_levels(T, src, b, Lay.buf0, Lay.buf1, fstride, Lay.ops, staged_src,
+                                    &s_bar, &bar_phase)) {
+                    if (threadIdx.x == 0) atomicExch(A.error, RT_ETIMEOUT);
+                }
                 mark(kPhLevels);
                 if (last) {
                     if (snr_tpr(b) == 8)
@@ -771,7 +874,8 @@ static int plan_prepare_device(SearchPlan& P)
     RT_TRY(dalloc(&P.d_scratch, (size_t)kSlots * 2 * std::max<size_t>(P.slot_floats, 1)));
     RT_TRY(dalloc(&P.d_counters, (size_t)P.nseq * kMaxStages + kSlots + 1));
     RT_TRY(dalloc(&P.d_ticket, 1));
-    RT_TRY(dalloc(&P.d_ds, P.ds_total));
+    // + 16 floats: bulk copies read whole 16-byte units around a block of rows
+    RT_TRY(dalloc(&P.d_ds, P.ds_total + 16));
     if (P.cfg.deredden) {
         RT_TRY(dalloc(&P.d_y, P.total_len));
         RT_TRY(dalloc(&P.d_rmed, P.scrunch > 1 ? P.lo_total : P.total_len));
@@ -1049,8 +1153,8 @@ extern "C" int rt_search_set_profiling(rt_search_plan* plan, int enable)
     if (!plan) return set_error(RT_EINVAL, "null argument");
     SearchPlan& P = plan->p;
     if (enable && !P.d_phase) {
-        RT_TRY_CUDA(cudaMalloc((void**)&P.d_phase, kPhases * sizeof(unsigned long long)));
-        RT_TRY_CUDA(cudaMemset(P.d_phase, 0, kPhases * sizeof(unsigned long long)));
+        RT_TRY_CUDA(cudaMalloc((void**)&P.d_phase, kCounters * sizeof(unsigned long long)));
+        RT_TRY_CUDA(cudaMemset(P.d_phase, 0, kCounters * sizeof(unsigned long long)));
     } else if (!enable && P.d_phase) {
         cudaFree(P.d_phase);
         P.d_phase = nullptr;
@@ -1064,8 +1168,8 @@ extern "C" int rt_search_phase_cycles(rt_search_plan* plan, uint64_t* h_cycles, 
     SearchPlan& P = plan->p;
     if (!P.d_phase) return set_error(RT_EINVAL, "profiling is not enabled on this plan");
     RT_TRY_CUDA(cudaDeviceSynchronize());
-    RT_TRY_CUDA(cudaMemcpy(h_cycles, P.d_phase, kPhases * sizeof(uint64_t), cudaMemcpyDeviceToHost));
-    if (reset) RT_TRY_CUDA(cudaMemset(P.d_phase, 0, kPhases * sizeof(unsigned long long)));
+    RT_TRY_CUDA(cudaMemcpy(h_cycles, P.d_phase, kCounters * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    if (reset) RT_TRY_CUDA(cudaMemset(P.d_phase, 0, kCounters * sizeof(unsigned long long)));
     return RT_OK;
 }
 

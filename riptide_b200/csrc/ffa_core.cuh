@@ -19,6 +19,7 @@
 // bit-identical to cpp/transforms.hpp.
 #pragma once
 #include "common.cuh"
+#include "bulk_copy.cuh"
 
 namespace rt {
 
@@ -160,8 +161,15 @@ __device__ __forceinline__ int find_node(const Node* nodes, int n, int r)
     return lo;
 }
 
-// Row stride of the level buffers (16-byte aligned rows).
-RT_HD int ffa_stride(int b) { return (b + 3) & ~3; }
+// Level rows in shared memory. When halo_mode(b), a row of b values is followed by a copy of
+// its first kHalo values, so a lane reading a rolled row at (p0 + 0..63) with p0 < b never
+// wraps; rows are 16-byte aligned either way. Halo mode covers the bins ranges of the usual
+// searches (bins_min 240 or 480): there the level loops are unrolled for exactly ceil(b / 64)
+// column pairs per lane (4, 5, 8, 9) and the global level for ceil(b / 32) columns
+// (8, 9, 15, 16, 17).
+constexpr int kHalo = 64;
+RT_HD bool halo_mode(int b) { return (b >= 225 && b <= 288) || (b >= 449 && b <= 544); }
+RT_HD int ffa_stride(int b) { return halo_mode(b) ? ((b + kHalo + 3) & ~3) : ((b + 3) & ~3); }
 
 // One output row of a level: out = row h + roll(row t, -shift) of the level below.
 // For the level read from global memory, h and t are global row indices; t < 0 marks a
@@ -249,6 +257,46 @@ __device__ __forceinline__ void level_rows_unrolled(const RowOp* ops, int nrows,
             const int c = lane + 32 * j;
             if (j < NIT - 1 || c < b) out[c] = v[j];
         }
+        if (halo_mode(b)) {  // columns 0..63 again after column b - 1 (NIT >= 2 here)
+            out[b + lane] = v[0];
+            out[b + 32 + lane] = v[1];
+        }
+    }
+}
+
+// Shared-memory level in halo mode: each lane computes column pairs (2 lane, 2 lane + 1) of
+// 64-column chunks. The rolled row is read from p0 = (64 j + shift) mod b on, which the halo
+// keeps in bounds without a per-element wrap. For odd b the last pair computes one column past
+// b - 1 into the halo position, which the halo stores below overwrite.
+template <int NIT2>
+__device__ __forceinline__ void level_rows_pairs(const RowOp* ops, int nrows,
+                                                 const float* __restrict__ src,
+                                                 float* __restrict__ dst, int stride, int b)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int r = warp; r < nrows; r += kWarps) {
+        const RowOp op = ops[r];
+        float* out = dst + (size_t)r * stride;
+        const float* H = src + (size_t)op.h * stride;
+        const float* Tr = src + (size_t)op.t * stride + 2 * lane;
+        float2 first = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int j = 0; j < NIT2; ++j) {
+            const int c = 64 * j + 2 * lane;
+            if (j < NIT2 - 1 || c < b) {
+                int p0 = op.shift + 64 * j;  // < b + 64 j: at most two wraps for NIT2 <= 9
+                p0 -= (p0 >= b) ? b : 0;
+                p0 -= (p0 >= b) ? b : 0;
+                const float2 h = *reinterpret_cast<const float2*>(H + c);
+                float2 o;
+                o.x = __fadd_rn(h.x, Tr[p0]);
+                o.y = __fadd_rn(h.y, Tr[p0 + 1]);
+                *reinterpret_cast<float2*>(out + c) = o;
+                if (j == 0) first = o;
+            }
+        }
+        out[b + 2 * lane] = first.x;
+        out[b + 2 * lane + 1] = first.y;
     }
 }
 
@@ -282,6 +330,14 @@ template <bool kGlobal>
 __device__ __forceinline__ void level_rows(const RowOp* ops, int nrows, const float* src,
                                            int sstride, float* dst, int stride, int b)
 {
+    if (!kGlobal && halo_mode(b)) {
+        switch ((b + 63) >> 6) {
+            case 4: level_rows_pairs<4>(ops, nrows, src, dst, stride, b); return;
+            case 5: level_rows_pairs<5>(ops, nrows, src, dst, stride, b); return;
+            case 8: level_rows_pairs<8>(ops, nrows, src, dst, stride, b); return;
+            default: level_rows_pairs<9>(ops, nrows, src, dst, stride, b); return;
+        }
+    }
     const int nit = (b + 31) >> 5;
     switch (nit) {
 #define RT_NIT_CASE(N) \
@@ -297,21 +353,51 @@ __device__ __forceinline__ void level_rows(const RowOp* ops, int nrows, const fl
 // `stride`, row i of the buffer = root output row lo + i). `src` is the global source:
 // row j of it is at src + j * b (j in transform row indexing). `ops` has room for the
 // largest level.
-__device__ inline void run_job_levels(const JobTree& T, const float* __restrict__ src, int b,
-                                      float* buf0, float* buf1, int stride, RowOp* ops)
+// Level computed from source rows staged in shared memory (packed, stride b): same loop as
+// the global level, plain loads.
+__device__ __forceinline__ void level_rows_staged(const RowOp* ops, int nrows, const float* src,
+                                                  float* dst, int stride, int b)
+{
+    switch ((b + 31) >> 5) {
+        case 8: level_rows_unrolled<8, false>(ops, nrows, src, b, dst, stride, b); break;
+        case 9: level_rows_unrolled<9, false>(ops, nrows, src, b, dst, stride, b); break;
+        case 15: level_rows_unrolled<15, false>(ops, nrows, src, b, dst, stride, b); break;
+        case 16: level_rows_unrolled<16, false>(ops, nrows, src, b, dst, stride, b); break;
+        case 17: level_rows_unrolled<17, false>(ops, nrows, src, b, dst, stride, b); break;
+        default: level_rows_generic<false>(ops, nrows, src, b, dst, stride, b);
+    }
+}
+
+// `staged` (optional): the job's source rows already being copied into shared memory, as a
+// pointer such that global row j of the source is at staged + j * b; the copy completes on
+// phase `*phase` of `bar`. Returns false if that wait ran out.
+__device__ inline bool run_job_levels(const JobTree& T, const float* __restrict__ src, int b,
+                                      float* buf0, float* buf1, int stride, RowOp* ops,
+                                      const float* staged = nullptr, uint64_t* bar = nullptr,
+                                      uint32_t* phase = nullptr)
 {
     build_all_ops(T, b, ops);
     cta_sync();
+    bool ok = true;
+    if (staged) {
+        ok = mbar_wait(bar, *phase);
+        *phase ^= 1u;
+    }
     for (int d = T.depth; d >= 0; --d) {
         float* dst = (d & 1) ? buf1 : buf0;
         const float* prev = (d & 1) ? buf0 : buf1;  // level d+1
         const RowOp* lops = ops + T.op_start[d];
-        if (d == T.depth)
-            level_rows<true>(lops, T.level_rows[d], src, b, dst, stride, b);
-        else
+        if (d == T.depth) {
+            if (staged)
+                level_rows_staged(lops, T.level_rows[d], staged, dst, stride, b);
+            else
+                level_rows<true>(lops, T.level_rows[d], src, b, dst, stride, b);
+        } else {
             level_rows<false>(lops, T.level_rows[d], prev, stride, dst, stride, b);
+        }
         cta_sync();
     }
+    return ok;
 }
 
 // Writes the root rows held in buf0 to global rows (root_row0 + s) of `dst` (stride b).
