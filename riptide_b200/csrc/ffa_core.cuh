@@ -161,15 +161,12 @@ __device__ __forceinline__ int find_node(const Node* nodes, int n, int r)
     return lo;
 }
 
-// Level rows in shared memory. When halo_mode(b), a row of b values is followed by a copy of
-// its first kHalo values, so a lane reading a rolled row at (p0 + 0..63) with p0 < b never
-// wraps; rows are 16-byte aligned either way. Halo mode covers the bins ranges of the usual
-// searches (bins_min 240 or 480): there the level loops are unrolled for exactly ceil(b / 64)
-// column pairs per lane (4, 5, 8, 9) and the global level for ceil(b / 32) columns
+// Level rows in shared memory: b values, 16-byte aligned rows. For the bins ranges of the
+// usual searches (bins_min 240 or 480) the level loops are unrolled for exactly ceil(b / 64)
+// two-column chunks per lane (4, 5, 8, 9) and the global level for ceil(b / 32) columns
 // (8, 9, 15, 16, 17).
-constexpr int kHalo = 64;
 RT_HD bool halo_mode(int b) { return (b >= 225 && b <= 288) || (b >= 449 && b <= 544); }
-RT_HD int ffa_stride(int b) { return halo_mode(b) ? ((b + kHalo + 3) & ~3) : ((b + 3) & ~3); }
+RT_HD int ffa_stride(int b) { return (b + 3) & ~3; }
 
 // One output row of a level: out = row h + roll(row t, -shift) of the level below.
 // For the level read from global memory, h and t are global row indices; t < 0 marks a
@@ -257,17 +254,12 @@ __device__ __forceinline__ void level_rows_unrolled(const RowOp* ops, int nrows,
             const int c = lane + 32 * j;
             if (j < NIT - 1 || c < b) out[c] = v[j];
         }
-        if (halo_mode(b)) {  // columns 0..63 again after column b - 1 (NIT >= 2 here)
-            out[b + lane] = v[0];
-            out[b + 32 + lane] = v[1];
-        }
     }
 }
 
-// Shared-memory level in halo mode: each lane computes column pairs (2 lane, 2 lane + 1) of
-// 64-column chunks. The rolled row is read from p0 = (64 j + shift) mod b on, which the halo
-// keeps in bounds without a per-element wrap. For odd b the last pair computes one column past
-// b - 1 into the halo position, which the halo stores below overwrite.
+// Shared-memory level for the usual bins ranges: in each 64-column chunk a lane computes
+// columns (64 j + lane) and (64 j + 32 + lane), so every load and store of the warp touches
+// 32 consecutive words (mod b); the rolled row is read from p0 = (64 j + shift) mod b on.
 template <int NIT2>
 __device__ __forceinline__ void level_rows_pairs(const RowOp* ops, int nrows,
                                                  const float* __restrict__ src,
@@ -277,26 +269,21 @@ __device__ __forceinline__ void level_rows_pairs(const RowOp* ops, int nrows,
     for (int r = warp; r < nrows; r += kWarps) {
         const RowOp op = ops[r];
         float* out = dst + (size_t)r * stride;
-        const float* H = src + (size_t)op.h * stride;
-        const float* Tr = src + (size_t)op.t * stride + 2 * lane;
-        float2 first = make_float2(0.f, 0.f);
+        const float* H = src + (size_t)op.h * stride + lane;
+        const float* Tr = src + (size_t)op.t * stride;
 #pragma unroll
         for (int j = 0; j < NIT2; ++j) {
-            const int c = 64 * j + 2 * lane;
-            if (j < NIT2 - 1 || c < b) {
-                int p0 = op.shift + 64 * j;  // < b + 64 j: at most two wraps for NIT2 <= 9
-                p0 -= (p0 >= b) ? b : 0;
-                p0 -= (p0 >= b) ? b : 0;
-                const float2 h = *reinterpret_cast<const float2*>(H + c);
-                float2 o;
-                o.x = __fadd_rn(h.x, Tr[p0]);
-                o.y = __fadd_rn(h.y, Tr[p0 + 1]);
-                *reinterpret_cast<float2*>(out + c) = o;
-                if (j == 0) first = o;
-            }
+            int p0 = op.shift + 64 * j;  // < b + 64 j: at most two wraps for NIT2 <= 9
+            p0 -= (p0 >= b) ? b : 0;
+            p0 -= (p0 >= b) ? b : 0;
+            const int c = 64 * j + lane;
+            int i0 = p0 + lane;
+            i0 -= (i0 >= b) ? b : 0;
+            int i1 = i0 + 32;
+            i1 -= (i1 >= b) ? b : 0;
+            if (j < NIT2 - 1 || c < b) out[c] = __fadd_rn(H[64 * j], Tr[i0]);
+            if (j < NIT2 - 1 || c + 32 < b) out[c + 32] = __fadd_rn(H[64 * j + 32], Tr[i1]);
         }
-        out[b + 2 * lane] = first.x;
-        out[b + 2 * lane + 1] = first.y;
     }
 }
 
