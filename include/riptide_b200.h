@@ -171,13 +171,15 @@ int rt_search_set_timing(rt_search_plan* plan, int enable);
  * h_ms[1] downsampling of all cycles, h_ms[2] the persistent FFA + S/N kernel; also the number
  * of kernel launches the run made. Synchronises with the run. */
 int rt_search_last_timing(rt_search_plan* plan, float* h_ms, int* h_launches);
-/* In-kernel profile of the persistent FFA kernel (12 entries): summed SM cycles of compute
+/* In-kernel profile of the persistent FFA kernel (16 entries): summed SM cycles of compute
  * thread 0 of every CTA in each phase of a work item (0 boxcar setup, 1 slot hand-over wait,
  * 2 job tree, 3 FFA levels, 4 S/N + periodogram rows, 5 stage output + counters, 6 item
  * decode), 7 cycles the scheduling warps spent choosing items; counts: 8 items blocked on a
- * scratch slot, 9 items blocked on a previous stage, 10 items claimed, 11 empty polls. */
+ * scratch slot, 9 items blocked on a previous stage, 10 items claimed, 11 empty polls,
+ * 12 values computed by FFA levels (rows x bins), 13 FFA levels run, 14 root rows produced,
+ * 15 items of stages after the first. */
 int rt_search_set_profiling(rt_search_plan* plan, int enable);
-int rt_search_phase_cycles(rt_search_plan* plan, uint64_t* h_cycles12, int reset);
+int rt_search_phase_cycles(rt_search_plan* plan, uint64_t* h_counters16, int reset);
 void rt_search_plan_destroy(rt_search_plan* plan);
 
 #ifdef __cplusplus

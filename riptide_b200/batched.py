@@ -131,11 +131,12 @@ class BatchedSearch(object):
 
     def phase_cycles(self, reset=True):
         """{phase: summed SM cycles} of the runs since the last reset."""
-        c = np.zeros(12, dtype=np.uint64)
+        c = np.zeros(16, dtype=np.uint64)
         _lib.check(_lib.load().rt_search_phase_cycles(self._plan, c.ctypes.data_as(_lib._u64p),
                                                       int(bool(reset))))
         names = ["fetch", "wait", "tree", "levels", "snr", "store", "decode", "sched_wait",
-                 "blocked_slot", "blocked_stage", "claimed", "empty_polls"]
+                 "blocked_slot", "blocked_stage", "claimed", "empty_polls", "level_values",
+                 "levels_run", "root_rows", "later_stage_items"]
         return {n: int(c[i]) for i, n in enumerate(names)}
 
     def close(self):

@@ -81,7 +81,7 @@ struct EngineArgs {
 enum { kPhFetch = 0, kPhWait, kPhTree, kPhLevels, kPhSnr, kPhStore, kPhases = 8 };
 // extra counters after the phases: blocked on a scratch slot, blocked on a previous stage,
 // items claimed, scheduler polls that found nothing ready
-constexpr int kCounters = 12;
+constexpr int kCounters = 16;
 
 __device__ __forceinline__ int ld_acquire(const int* p)
 {
@@ -290,6 +290,7 @@ __global__ void __launch_bounds__(kEngineThreads, 1) k_search_persistent(EngineA
     uint32_t bar_phase = 0;
     const bool prof = A.phase_cycles != nullptr;
     unsigned long long ph[kPhases] = {0, 0, 0, 0, 0, 0, 0, 0};
+    unsigned long long cnt[4] = {0, 0, 0, 0};  // counters 12..15
     long long tprev = prof ? clock64() : 0;
     auto mark = [&](int phase) {
         if (prof && threadIdx.x == 0) {
@@ -353,6 +354,13 @@ __global__ void __launch_bounds__(kEngineThreads, 1) k_search_persistent(EngineA
                 }
             } else {
                 mark(kPhTree);
+                if (prof && threadIdx.x == 0) {
+                    for (int d = 0; d <= T.depth; ++d)
+                        cnt[0] += (unsigned long long)T.level_rows[d] * b;
+                    cnt[1] += T.depth + 1;
+                    cnt[2] += J.hi - J.lo;
+                    cnt[3] += stage > 0;
+                }
                 if (!run_job_levels(T, src, b, Lay.buf0, Lay.buf1, fstride, Lay.ops, staged_src,
                                     &s_bar, &bar_phase)) {
                     if (threadIdx.x == 0) atomicExch(A.error, RT_ETIMEOUT);
@@ -385,6 +393,8 @@ __global__ void __launch_bounds__(kEngineThreads, 1) k_search_persistent(EngineA
     }
     if (prof && threadIdx.x == 0)
         for (int i = 0; i < kPhases; ++i) atomicAdd(A.phase_cycles + i, ph[i]);
+    if (prof && threadIdx.x == 0)
+        for (int i = 0; i < 4; ++i) atomicAdd(A.phase_cycles + 12 + i, cnt[i]);
 }
 
 // ------------------------------------------------------------------------------------
@@ -1162,13 +1172,13 @@ extern "C" int rt_search_set_profiling(rt_search_plan* plan, int enable)
     return RT_OK;
 }
 
-extern "C" int rt_search_phase_cycles(rt_search_plan* plan, uint64_t* h_cycles, int reset)
+extern "C" int rt_search_phase_cycles(rt_search_plan* plan, uint64_t* h_counters, int reset)
 {
-    if (!plan || !h_cycles) return set_error(RT_EINVAL, "null argument");
+    if (!plan || !h_counters) return set_error(RT_EINVAL, "null argument");
     SearchPlan& P = plan->p;
     if (!P.d_phase) return set_error(RT_EINVAL, "profiling is not enabled on this plan");
     RT_TRY_CUDA(cudaDeviceSynchronize());
-    RT_TRY_CUDA(cudaMemcpy(h_cycles, P.d_phase, kCounters * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    RT_TRY_CUDA(cudaMemcpy(h_counters, P.d_phase, kCounters * sizeof(uint64_t), cudaMemcpyDeviceToHost));
     if (reset) RT_TRY_CUDA(cudaMemset(P.d_phase, 0, kCounters * sizeof(unsigned long long)));
     return RT_OK;
 }
