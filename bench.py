@@ -286,32 +286,34 @@ def bench_ours(args):
                 "alg_bytes_per_launch": bytes_kernel}
 
     # ---- end to end through the public API with host buffers (rank 0 prints) ----
+    # SearchPipeline (C ABI rt_search_pipeline_*): host series in, host periodograms out, in
+    # chunks of trials whose copies overlap the search of the neighbouring chunks.
     e2e = None
     if not args.no_e2e:
-        host_in = data.cpu().pin_memory()
-        host_out = [torch.empty(o.shape, dtype=o.dtype, pin_memory=True) for o in outs]
-        dev_in = torch.empty_like(data)
+        pipe = rb.SearchPipeline(lengths, cfg["tsamp"], chunk_trials=args.chunk_trials,
+                                 **cfg["search"])
+        host_in, host_out = pipe.allocate_host()
+        host_in.copy_(data.cpu())
         h2d = host_in.numel() * 4
-        d2h = sum(o.numel() * o.element_size() for o in outs)
-        def e2e_step():
-            dev_in.copy_(host_in, non_blocking=True)
-            bs.run(dev_in, outs, check=False)
-            for h, o in zip(host_out, outs):
-                h.copy_(o, non_blocking=True)
-        e2e_step()
-        torch.cuda.synchronize()
+        d2h = sum(o.numel() * o.element_size() for o in host_out)
+        pipe.run(host_in, host_out, check=True)
         barrier(world)
+        torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
         for _ in range(max(1, args.e2e_steps)):
-            e2e_step()
+            pipe.run(host_in, host_out, check=False)
         b.record(stream)
         torch.cuda.synchronize()
+        pipe.check()
         ems = max_over_ranks(a.elapsed_time(b) / max(1, args.e2e_steps), world)
         e2e = {"value": ntrials * world / (ems * 1e-3), "unit": "trials/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "ms_per_step": ems}
-        del host_in, host_out, dev_in
+               "ms_per_step": ems, "api": "SearchPipeline (rt_search_pipeline_run), "
+               "page-locked host buffers, %d chunks of %d trials" % (pipe.num_chunks,
+                                                                      args.chunk_trials)}
+        pipe.close()
+        del host_in, host_out
 
     # ---- plain per-(cycle, bins) GPU path on a few trials, for the batching ratio ----
     plain = None
@@ -392,6 +394,7 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=64)
     ap.add_argument("--plain-trials", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--chunk-trials", type=int, default=32)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()

@@ -157,6 +157,9 @@ int rt_search_plan_create(const uint64_t* h_lengths, size_t ntrials,
 /* Row offsets of each trial in the packed outputs: ntrials + 1 entries. */
 int rt_search_plan_rows(const rt_search_plan* plan, uint64_t* h_row_offsets);
 int rt_search_plan_stats(const rt_search_plan* plan, rt_search_plan_stats_t* stats);
+/* Allocates and uploads the plan's device buffers now (otherwise the first run does it;
+ * cudaMalloc synchronises the device, so do this before timing or overlapping work). */
+int rt_search_plan_prepare(rt_search_plan* plan);
 /* Enqueues the search. d_data: the series packed back to back (plan order). Outputs are
  * packed by trial (rt_search_plan_rows). d_normalised (optional, may be NULL) receives the
  * dereddened + normalised series actually searched. Device buffers of the plan are
@@ -181,6 +184,34 @@ int rt_search_last_timing(rt_search_plan* plan, float* h_ms, int* h_launches);
 int rt_search_set_profiling(rt_search_plan* plan, int enable);
 int rt_search_phase_cycles(rt_search_plan* plan, uint64_t* h_counters16, int reset);
 void rt_search_plan_destroy(rt_search_plan* plan);
+
+/* ---------------------------------------------------------------------------------
+ * Host-buffer pipeline: the batched search of series in host memory, the way the
+ * reference's worker pool searches DM trials from host memory (pipeline/worker_pool.py:35-68
+ * calling search.py:11-93), with the copies in and out overlapped with the search. The
+ * trials are cut into chunks of at most `chunk_trials` consecutive trials (one plan each);
+ * while chunk i is searched, chunk i+1 is copied in and chunk i-1's periodograms are
+ * copied out. Host buffers must be page-locked for the copies to overlap.
+ * -------------------------------------------------------------------------------*/
+typedef struct rt_search_pipeline rt_search_pipeline;
+
+int rt_search_pipeline_create(const uint64_t* h_lengths, size_t ntrials,
+                              const rt_search_config* cfg, const uint64_t* h_widths,
+                              size_t num_widths, size_t chunk_trials,
+                              rt_search_pipeline** pipeline);
+/* Row offsets of each trial in the packed host outputs: ntrials + 1 entries. */
+int rt_search_pipeline_rows(const rt_search_pipeline* pipeline, uint64_t* h_row_offsets);
+int rt_search_pipeline_chunks(const rt_search_pipeline* pipeline, size_t* h_nchunks);
+/* Enqueues the search of h_data (series packed back to back) into the host outputs, packed
+ * by trial: h_periods f64[L], h_foldbins u32[L], h_snrs f32[L * num_widths]. The work runs
+ * after what is already queued on `stream`, and `stream` waits for its end. Returns once
+ * enqueued; the host outputs are complete after rt_search_pipeline_check. */
+int rt_search_pipeline_run(rt_search_pipeline* pipeline, const float* h_data,
+                           double* h_periods, uint32_t* h_foldbins, float* h_snrs,
+                           void* stream);
+/* Synchronises `stream` and reports a device-side failure of any chunk. */
+int rt_search_pipeline_check(rt_search_pipeline* pipeline, void* stream);
+void rt_search_pipeline_destroy(rt_search_pipeline* pipeline);
 
 #ifdef __cplusplus
 }

@@ -4,7 +4,7 @@ Hand-written sm_100a CUDA kernels behind a C ABI (include/riptide_b200.h), with 
 reference's Python API on top. ``riptide_b200.libcpp`` replaces ``riptide.libcpp``.
 """
 from . import libcpp
-from .batched import BatchedSearch, ffa_search_batched
+from .batched import BatchedSearch, SearchPipeline, ffa_search_batched
 from .ffautils import generate_width_trials
 from .libffa import boxcar_snr, downsample, ffa1, ffa2, ffafreq, ffaprd, generate_signal
 from .periodogram import Periodogram
@@ -13,7 +13,8 @@ from .search import ffa_search
 from .time_series import TimeSeries
 
 __all__ = [
-    "TimeSeries", "Periodogram", "ffa_search", "ffa_search_batched", "BatchedSearch", "ffa1",
+    "TimeSeries", "Periodogram", "ffa_search", "ffa_search_batched", "BatchedSearch", "SearchPipeline",
+    "ffa1",
     "ffa2", "ffafreq", "ffaprd", "generate_signal", "downsample", "boxcar_snr",
     "running_median", "fast_running_median", "generate_width_trials", "libcpp",
 ]

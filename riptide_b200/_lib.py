@@ -50,6 +50,13 @@ SIGNATURES = {
     "rt_search_set_profiling": (ctypes.c_int, [_vp, ctypes.c_int]),
     "rt_search_phase_cycles": (ctypes.c_int, [_vp, _u64p, ctypes.c_int]),
     "rt_search_plan_destroy": (None, [_vp]),
+    "rt_search_plan_prepare": (ctypes.c_int, [_vp]),
+    "rt_search_pipeline_create": (ctypes.c_int, [_u64p, _sz, _vp, _u64p, _sz, _sz, ctypes.POINTER(_vp)]),
+    "rt_search_pipeline_rows": (ctypes.c_int, [_vp, _u64p]),
+    "rt_search_pipeline_chunks": (ctypes.c_int, [_vp, ctypes.POINTER(_sz)]),
+    "rt_search_pipeline_run": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "rt_search_pipeline_check": (ctypes.c_int, [_vp, _vp]),
+    "rt_search_pipeline_destroy": (None, [_vp]),
 }
 
 

@@ -160,3 +160,134 @@ def ffa_search_batched(series, tsamp, **kwargs):
         return bs.search(series)
     finally:
         bs.close()
+
+
+def _host_ptr(a, dtypes, n, name):
+    """Address of a contiguous host buffer (numpy array or CPU torch tensor) of n values of
+    one of `dtypes` (numpy dtype names)."""
+    if hasattr(a, "data_ptr") and hasattr(a, "is_cuda"):
+        if a.is_cuda:
+            raise ValueError(f"{name} must be in host memory")
+        ok = a.is_contiguous() and a.numel() == n and str(a.dtype).replace("torch.", "") in dtypes
+        ptr = a.data_ptr()
+    else:
+        ok = (isinstance(a, np.ndarray) and a.dtype.name in dtypes and a.flags.c_contiguous
+              and a.size == n)
+        ptr = a.ctypes.data if ok else 0
+    if not ok:
+        raise ValueError(f"{name} must be a contiguous host buffer of {n} {dtypes[0]}")
+    return ptr
+
+
+class SearchPipeline(object):
+    """Batched search of series held in host memory (C ABI rt_search_pipeline_*).
+
+    The trials are cut into chunks of ``chunk_trials`` consecutive trials; the copy of chunk
+    i+1 to the GPU and the copy of chunk i-1's periodograms back to the host overlap the
+    search of chunk i. Host buffers from ``allocate_host`` are page-locked, which the
+    overlap needs. Same outputs as ``BatchedSearch`` (every trial is searched independently).
+    """
+
+    def __init__(self, lengths, tsamp, chunk_trials=64, period_min=1.0, period_max=30.0,
+                 bins_min=240, bins_max=260, ducy_max=0.20, wtsp=1.5, deredden=True,
+                 rmed_width=4.0, rmed_minpts=101, already_normalised=False, widths=None):
+        self.lengths = np.ascontiguousarray(np.asarray(lengths, dtype=np.uint64).ravel())
+        self.tsamp = float(tsamp)
+        self.widths = (np.asarray(widths) if widths is not None
+                       else generate_width_trials(bins_min, ducy_max=ducy_max, wtsp=wtsp))
+        cfg = _lib.SearchConfig(
+            tsamp=self.tsamp, period_min=float(period_min), period_max=float(period_max),
+            bins_min=int(bins_min), bins_max=int(bins_max), deredden=int(bool(deredden)),
+            rmed_width=float(rmed_width), rmed_minpts=int(rmed_minpts),
+            already_normalised=int(bool(already_normalised)))
+        w, wp = _lib.u64_array(self.widths)
+        h = ctypes.c_void_p()
+        _lib.check(_lib.load().rt_search_pipeline_create(
+            self.lengths.ctypes.data_as(_lib._u64p), self.lengths.size, ctypes.byref(cfg), wp,
+            w.size, int(chunk_trials), ctypes.byref(h)))
+        self._pipe = h
+        rows = np.zeros(self.lengths.size + 1, dtype=np.uint64)
+        _lib.check(_lib.load().rt_search_pipeline_rows(h, rows.ctypes.data_as(_lib._u64p)))
+        self.row_offsets = rows.astype(np.int64)
+        n = ctypes.c_size_t(0)
+        _lib.check(_lib.load().rt_search_pipeline_chunks(h, ctypes.byref(n)))
+        self.num_chunks = int(n.value)
+        self.sample_offsets = np.concatenate([[0], np.cumsum(self.lengths.astype(np.int64))])
+
+    @property
+    def num_trials(self):
+        return int(self.lengths.size)
+
+    @property
+    def total_rows(self):
+        return int(self.row_offsets[-1])
+
+    def allocate_host(self):
+        """Page-locked host buffers: (input f32[samples], periods f64[L], foldbins i32[L],
+        snrs f32[L, nw]) as CPU torch tensors."""
+        torch = libcpp._t()
+        L, nw = self.total_rows, self.widths.size
+        return (torch.empty((int(self.sample_offsets[-1]),), dtype=torch.float32, pin_memory=True),
+                (torch.empty((L,), dtype=torch.float64, pin_memory=True),
+                 torch.empty((L,), dtype=torch.int32, pin_memory=True),
+                 torch.empty((L, nw), dtype=torch.float32, pin_memory=True)))
+
+    def run(self, host_data, host_outputs, check=True):
+        """Search host_data (all series packed back to back) into host_outputs (periods,
+        foldbins, snrs). Enqueued after the current torch stream's work; `check` waits for
+        the results and raises on a device-side failure."""
+        L, nw = self.total_rows, int(self.widths.size)
+        periods, foldbins, snrs = host_outputs
+        pd = _host_ptr(host_data, ("float32",), int(self.sample_offsets[-1]), "host_data")
+        pp = _host_ptr(periods, ("float64",), L, "periods")
+        pf = _host_ptr(foldbins, ("int32", "uint32"), L, "foldbins")
+        ps = _host_ptr(snrs, ("float32",), L * nw, "snrs")
+        st = libcpp._stream()
+        _lib.check(_lib.load().rt_search_pipeline_run(self._pipe, ctypes.c_void_p(pd),
+                                                      ctypes.c_void_p(pp), ctypes.c_void_p(pf),
+                                                      ctypes.c_void_p(ps), st))
+        if check:
+            self.check()
+        return host_outputs
+
+    def check(self):
+        """Wait for the last run and raise on a device-side failure."""
+        _lib.check(_lib.load().rt_search_pipeline_check(self._pipe, libcpp._stream()))
+
+    def search(self, series):
+        """Search host series (list of 1D arrays, or one packed array); a list of
+        Periodogram."""
+        host_in, outs = self.allocate_host()
+        x = host_in.numpy()
+        if isinstance(series, np.ndarray) and series.ndim == 1:
+            if series.size != x.size:
+                raise ValueError("series lengths do not match the plan")
+            x[:] = series
+        else:
+            if len(series) != self.num_trials:
+                raise ValueError("series lengths do not match the plan")
+            for i, s in enumerate(series):
+                s = np.asarray(s, dtype=np.float32).ravel()
+                if s.size != self.lengths[i]:
+                    raise ValueError("series lengths do not match the plan")
+                x[self.sample_offsets[i]:self.sample_offsets[i + 1]] = s
+        self.run(host_in, outs)
+        p, fb, s = outs[0].numpy(), outs[1].numpy().view(np.uint32), outs[2].numpy()
+        out = []
+        for i in range(self.num_trials):
+            a, b = self.row_offsets[i], self.row_offsets[i + 1]
+            md = {"tobs": float(self.lengths[i]) * self.tsamp}
+            out.append(Periodogram(self.widths, p[a:b].copy(), fb[a:b].copy(), s[a:b].copy(),
+                                   metadata=md))
+        return out
+
+    def close(self):
+        if getattr(self, "_pipe", None):
+            _lib.load().rt_search_pipeline_destroy(self._pipe)
+            self._pipe = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

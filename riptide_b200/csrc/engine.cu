@@ -1130,6 +1130,12 @@ extern "C" int rt_search_run(rt_search_plan* plan, const float* data, float* nor
     return plan_run(plan->p, data, normalised_out, periods, foldbins, snrs, st);
 }
 
+extern "C" int rt_search_plan_prepare(rt_search_plan* plan)
+{
+    if (!plan) return set_error(RT_EINVAL, "null argument");
+    return plan_prepare_device(plan->p);
+}
+
 extern "C" int rt_search_check(rt_search_plan* plan, void* stream)
 {
     if (!plan) return set_error(RT_EINVAL, "null argument");

@@ -256,3 +256,26 @@ def test_batched_full_size_trial(rb):
     z, widths, p, fb, sn = O.ffa_search(x, 64e-6, period_min=0.2, period_max=30.0)
     assert np.allclose(zs[0], z, rtol=1e-5, atol=1e-5)
     _check_pgram(pgs[0].periods, pgs[0].foldbins, pgs[0].snrs, p, fb, sn, rtol=1e-4, atol=1e-4)
+
+
+def test_pipeline_equals_batched(rb):
+    # host-buffer pipeline (3 chunks, so both device buffer pairs are reused) against the
+    # device-resident batched search of the same trials: identical outputs
+    rng = np.random.default_rng(78)
+    lengths = [70001, 65536, 90000, 50000, 81234]
+    series = [rb.generate_signal(n, 0.9 / 5e-4 + 11 * i, ducy=0.04, amplitude=12.0, rng=rng)
+              .astype(np.float32) + 0.25 for i, n in enumerate(lengths)]
+    kw = dict(period_min=0.2, period_max=3.0, bins_min=240, bins_max=260, rmed_width=1.0)
+    pipe = rb.SearchPipeline(lengths, 5e-4, chunk_trials=2, **kw)
+    assert pipe.num_chunks == 3
+    for _ in range(2):  # second run reuses every buffer and event
+        pgs = pipe.search(series)
+    ref = rb.ffa_search_batched(series, 5e-4, **kw)
+    for a, b in zip(pgs, ref):
+        assert np.array_equal(a.periods, b.periods)
+        assert np.array_equal(a.foldbins, b.foldbins)
+        assert np.array_equal(a.snrs, b.snrs)
+    host_in, outs = pipe.allocate_host()
+    with pytest.raises(ValueError):
+        pipe.run(host_in[:-1], outs)
+    pipe.close()
