@@ -182,6 +182,7 @@ static int downsample_one(const float* d_in, size_t size, double f, float* d_out
     job.ncycles = 1;
     const int use_seg = h.use_seg, skip = 0;
     job.use_seg_host = &use_seg;
+    job.f_host = &f;
     job.skip_host = &skip;
     int s = launch_downsample(job, 1, size, st);
     cudaFreeAsync(d, st);

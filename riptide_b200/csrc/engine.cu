@@ -429,11 +429,60 @@ __global__ void k_scrunch(const float* __restrict__ x, TrialArrays A, int k,
 
 constexpr int kStatThreads = 256;
 
+// Unsigned 32-bit division by an invariant divisor d >= 1 with one multiply-high
+// (Granlund & Montgomery, "Division by invariant integers using multiplication", PLDI 1994,
+// figure 4.1): l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1,
+// q = (t + ((n - t) >> min(l, 1))) >> max(l - 1, 0) with t = mulhi(m, n); exact for every
+// 32-bit n.
+struct DivMagic {
+    unsigned m;
+    int sh1, sh2;
+};
+
+inline DivMagic div_magic(unsigned d)
+{
+    int l = 0;
+    while ((1ull << l) < d) ++l;
+    DivMagic g;
+    g.m = (unsigned)((((1ull << 32) * ((1ull << l) - d)) / d) + 1);
+    g.sh1 = l < 1 ? l : 1;
+    g.sh2 = l - 1 > 0 ? l - 1 : 0;
+    return g;
+}
+
+__device__ __forceinline__ unsigned div_by_magic(unsigned n, const DivMagic& g)
+{
+    const unsigned t = __umulhi(g.m, n);
+    return (t + ((n - t) >> g.sh1)) >> g.sh2;
+}
+
+// np.interp coefficients of the scrunched running median (running_medians.py:82-85):
+// coef[j] = (fp[j], (fp[j+1] - fp[j]) / k) in float64, so that the interpolated value at
+// x = j*k + (k-1)/2 + dx is fp[j] + slope * dx as numpy evaluates it.
+__global__ void k_interp_coef(TrialArrays A, int k, const float* __restrict__ rmed,
+                              double2* __restrict__ coef)
+{
+    const int trial = blockIdx.y;
+    const size_t nl = A.lo_len[trial];
+    const float* fp = rmed + A.lo_off[trial];
+    double2* c = coef + A.lo_off[trial];
+    for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < nl;
+         j += (size_t)gridDim.x * blockDim.x) {
+        const double a = (double)fp[j];
+        const double s = (j + 1 < nl) ? __ddiv_rn(__dsub_rn((double)fp[j + 1], a), (double)k) : 0.0;
+        c[j] = make_double2(a, s);
+    }
+}
+
 // y = float32(x - running median); per-block shifted sums for the statistics.
-// k > 1: rmed = np.interp(i, j*k + (k-1)/2, rmed_lores) in float64 (running_medians.py:82-85);
+// k > 1: rmed = np.interp(i, j*k + (k-1)/2, rmed_lores) in float64 (running_medians.py:82-85),
+// from the coefficients of k_interp_coef; with v = 2i - (k-1) = 2k*j + 2*dx, the segment j
+// and the offset dx = v mod 2k / 2 come from one invariant division (exact in 32 bits while
+// 2N < 2^32; longer series take 64-bit division);
 // k == 1: rmed is the full-resolution float32 running median (float32 subtraction).
 __global__ void __launch_bounds__(kStatThreads)
-    k_dered(const float* __restrict__ x, TrialArrays A, int k, const float* __restrict__ rmed,
+    k_dered(const float* __restrict__ x, TrialArrays A, int k, DivMagic g2k,
+            const float* __restrict__ rmed, const double2* __restrict__ coef,
             float* __restrict__ y, double* __restrict__ part, int blocks_per_trial)
 {
     const int trial = blockIdx.y;
@@ -441,8 +490,8 @@ __global__ void __launch_bounds__(kStatThreads)
     const float* xr = x + A.off[trial];
     float* yr = y + A.off[trial];
     const float* fp = rmed + (k > 1 ? A.lo_off[trial] : A.off[trial]);
+    const double2* cf = coef + (k > 1 ? A.lo_off[trial] : 0);
     const size_t nl = A.lo_len[trial];
-    const double half = 0.5 * (double)(k - 1);
     double s1 = 0.0, s2 = 0.0;
     const float shift = xr[0];
     float shift_y;
@@ -453,35 +502,38 @@ __global__ void __launch_bounds__(kStatThreads)
         else r0 = 0.0;
         shift_y = (k > 1) ? __double2float_rn((double)shift - r0) : __fsub_rn(shift, fp[0]);
     }
+    const double shift_yd = (double)shift_y;
+    // v = 2i - (k-1) ranges: v < 0 is left of xp[0]; v >= 2k(nl-1) is at or right of xp[-1]
+    const long long vlast = 2LL * k * (long long)(nl - 1);
+    const bool small = 2 * (unsigned long long)N < (1ull << 32);
+    const double first = (k > 1) ? (double)fp[0] : 0.0;
+    const double last = (k > 1) ? (double)fp[nl - 1] : 0.0;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N;
          i += (size_t)blocks_per_trial * blockDim.x) {
         const float xv = xr[i];
         float yv;
         if (k > 1) {
-            const double xi = (double)i;
+            const long long v = 2LL * (long long)i - (k - 1);
             double r;
-            const double x0 = half, xl = (double)(nl - 1) * k + half;
-            if (xi < x0) {
-                r = (double)fp[0];
-            } else if (xi >= xl) {
-                r = (double)fp[nl - 1];
+            if (v < 0) {
+                r = first;
+            } else if (v >= vlast) {
+                r = last;
             } else {
-                long long j = (2LL * (long long)i - (k - 1)) / (2LL * k);
-                const double xj = (double)j * k + half;
-                if (xj == xi) {
-                    r = (double)fp[j];
-                } else {
-                    const double slope =
-                        __ddiv_rn(__dsub_rn((double)fp[j + 1], (double)fp[j]), (double)k);
-                    r = __dadd_rn(__dmul_rn(slope, __dsub_rn(xi, xj)), (double)fp[j]);
-                }
+                long long j;
+                if (small) j = (long long)div_by_magic((unsigned)v, g2k);
+                else j = v / (2LL * k);
+                const int twodx = (int)(v - j * 2LL * k);  // 2 (x - xp[j]), 0 <= . < 2k
+                const double2 c = cf[j];
+                // x - xp[j] is exact in double; numpy's interp returns fp[j] at x == xp[j]
+                r = (twodx == 0) ? c.x : __dadd_rn(__dmul_rn(c.y, 0.5 * (double)twodx), c.x);
             }
             yv = __double2float_rn(__dsub_rn((double)xv, r));
         } else {
             yv = __fsub_rn(xv, fp[i]);
         }
         yr[i] = yv;
-        const double d = (double)yv - (double)shift_y;
+        const double d = (double)yv - shift_yd;
         s1 += d;
         s2 += d * d;
     }
@@ -651,6 +703,7 @@ struct SearchPlan {
     float* d_y = nullptr;               // dereddened series
     float* d_norm = nullptr;            // normalised copy (when a cycle has f == 1)
     float* d_lores = nullptr;
+    double2* d_coef = nullptr;          // interpolation coefficients of the running median
     float* d_rmed = nullptr;
     double* d_part = nullptr;
     double* d_mean = nullptr;
@@ -848,7 +901,7 @@ static int plan_build(SearchPlan& P)
 static void plan_free_device(SearchPlan& P)
 {
     void* ptrs[] = {P.d_widths, P.d_xforms, P.d_items, P.d_plans, P.d_scratch, P.d_counters,
-                    P.d_ticket, P.d_ds, P.d_y, P.d_norm, P.d_lores, P.d_rmed, P.d_part,
+                    P.d_ticket, P.d_ds, P.d_y, P.d_norm, P.d_lores, P.d_coef, P.d_rmed, P.d_part,
                     P.d_mean, P.d_normv, P.d_len, P.d_off, P.d_lo_len, P.d_lo_off, P.d_f,
                     P.d_useseg, P.d_dsoff};
     for (void* p : ptrs)
@@ -889,7 +942,10 @@ static int plan_prepare_device(SearchPlan& P)
     if (P.cfg.deredden) {
         RT_TRY(dalloc(&P.d_y, P.total_len));
         RT_TRY(dalloc(&P.d_rmed, P.scrunch > 1 ? P.lo_total : P.total_len));
-        if (P.scrunch > 1) RT_TRY(dalloc(&P.d_lores, P.lo_total));
+        if (P.scrunch > 1) {
+            RT_TRY(dalloc(&P.d_lores, P.lo_total));
+            RT_TRY(dalloc(&P.d_coef, P.lo_total));
+        }
     }
     if (P.has_unit_factor) RT_TRY(dalloc(&P.d_norm, P.total_len));
     RT_TRY(dalloc(&P.d_part, (size_t)T * P.stat_blocks * 3));
@@ -935,15 +991,18 @@ static int plan_run(SearchPlan& P, const float* data, float* normalised_out, dou
             RT_TRY_CUDA(cudaGetLastError());
             RT_TRY(launch_running_median(P.d_lores, P.d_lo_len, P.d_lo_off, T, P.max_lo,
                                          (int)P.cfg.rmed_minpts, P.d_rmed, st));
-            launches += 2;
+            dim3 gc((unsigned)std::min<size_t>((P.max_lo + 255) / 256, 1024), (unsigned)T);
+            k_interp_coef<<<gc, 256, 0, st>>>(TA, k, P.d_rmed, P.d_coef);
+            RT_TRY_CUDA(cudaGetLastError());
+            launches += 3;
         } else {
             RT_TRY(launch_running_median(data, P.d_len, P.d_off, T, P.max_len, P.rmed_width,
                                          P.d_rmed, st));
             launches += 1;
         }
         dim3 g((unsigned)P.stat_blocks, (unsigned)T);
-        k_dered<<<g, kStatThreads, 0, st>>>(data, TA, k, P.d_rmed, P.d_y, P.d_part,
-                                            P.stat_blocks);
+        k_dered<<<g, kStatThreads, 0, st>>>(data, TA, k, div_magic(2u * (unsigned)k), P.d_rmed,
+                                            P.d_coef, P.d_y, P.d_part, P.stat_blocks);
         RT_TRY_CUDA(cudaGetLastError());
         launches += 1;
         series = P.d_y;
@@ -981,6 +1040,7 @@ static int plan_run(SearchPlan& P, const float* data, float* normalised_out, dou
     job.out_off = P.d_dsoff;
     job.ncycles = C;
     job.use_seg_host = P.use_seg.data();
+    job.f_host = P.f.data();
     job.skip_host = P.skip.data();
     RT_TRY(launch_downsample(job, T, P.max_len, st));
     {
@@ -1288,6 +1348,7 @@ extern "C" int rt_deredden(const float* d_x, size_t size, double tsamp, double w
     TrialArrays A;
     RT_TRY(one_series_arrays(size, nl, &d, st, &A));
     float *lores = nullptr, *rmed = nullptr;
+    double2* coef = nullptr;
     double* part = nullptr;
     int s = RT_OK;
     const int blocks = 64;
@@ -1295,17 +1356,25 @@ extern "C" int rt_deredden(const float* d_x, size_t size, double tsamp, double w
     if (k > 1) {
         RT_TRY_CUDA(cudaMallocAsync((void**)&lores, nl * sizeof(float), st));
         RT_TRY_CUDA(cudaMallocAsync((void**)&rmed, nl * sizeof(float), st));
+        RT_TRY_CUDA(cudaMallocAsync((void**)&coef, nl * sizeof(double2), st));
         k_scrunch<<<dim3((unsigned)std::min<size_t>((nl * 32 + 255) / 256, 4096), 1), 256, 0, st>>>(
             d_x, A, k, lores);
         s = launch_running_median(lores, A.lo_len, A.lo_off, 1, nl, w, rmed, st);
+        if (s == RT_OK) {
+            k_interp_coef<<<dim3((unsigned)std::min<size_t>((nl + 255) / 256, 1024), 1), 256, 0, st>>>(
+                A, k, rmed, coef);
+            s = check_cuda(cudaGetLastError(), "deredden");
+        }
     } else {
         RT_TRY_CUDA(cudaMallocAsync((void**)&rmed, size * sizeof(float), st));
         s = launch_running_median(d_x, A.len, A.off, 1, size, w, rmed, st);
     }
     if (s == RT_OK) {
-        k_dered<<<dim3(blocks, 1), kStatThreads, 0, st>>>(d_x, A, k, rmed, d_out, part, blocks);
+        k_dered<<<dim3(blocks, 1), kStatThreads, 0, st>>>(d_x, A, k, div_magic(2u * (unsigned)k),
+                                                          rmed, coef, d_out, part, blocks);
         s = check_cuda(cudaGetLastError(), "deredden");
     }
+    if (coef) cudaFreeAsync(coef, st);
     if (lores) cudaFreeAsync(lores, st);
     if (rmed) cudaFreeAsync(rmed, st);
     cudaFreeAsync(part, st);

@@ -304,12 +304,16 @@ int snr2(const float* x, size_t rows, size_t cols, const int* d_widths, const in
 // Downsampling by a real factor (downsample.hpp:44-82).
 //
 // One CTA owns the output samples whose first input sample imin = floor(k f) falls in its
-// segment [seg0, seg0 + kDsSeg). It stages the segment plus a halo in shared memory with
+// segment [seg0, seg0 + seg). It stages kDsStage samples from seg0 (the segment plus a halo
+// of at least f + 1 samples for the largest factor f of the run) in shared memory with
 // an exclusive prefix sum in double, so each output costs O(1):
 //   out[k] = wmin*z[imin] + (P[imax] - P[imin+1]) + wmax*z[imax]
 // with the reference's FP64 sample bounds and float32 edge weights; the sum is formed in
-// double and rounded once. All cycles of a search are produced in the same pass, so the
-// series is read once. Factors with f + 2 > kDsHalo use k_downsample_wide instead.
+// double and rounded once. When the series is normalised on the way ((v - mean) / norm,
+// time_series.py:84-93), the weighted sum of the raw values is normalised instead:
+// (acc - mean * W) / norm with W the total weight, one rounding instead of one per sample.
+// All cycles of a search are produced in the same pass, so the series is read once.
+// Factors with f + 2 > kDsHalo use k_downsample_wide instead.
 // ------------------------------------------------------------------------------------
 __device__ __forceinline__ size_t first_k_at_or_after(size_t i0, double f)
 {
@@ -320,7 +324,12 @@ __device__ __forceinline__ size_t first_k_at_or_after(size_t i0, double f)
     return k;
 }
 
-__global__ void __launch_bounds__(512)
+constexpr int kDsThreads = 512;
+constexpr int kDsWarps = kDsThreads / 32;
+constexpr int kDsPerWarp = kDsStage / kDsWarps;  // staged samples per warp
+constexpr int kDsChunks = kDsPerWarp / 32;       // 32-sample chunks per warp
+
+__global__ void __launch_bounds__(kDsThreads, 2)
     k_downsample_segments(DsJob job)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -328,68 +337,47 @@ __global__ void __launch_bounds__(512)
     float* zs = reinterpret_cast<float*>(P + kDsStage + 1);          // kDsStage
     __shared__ int s_cnt[kDsMaxCycles + 1];
     __shared__ size_t s_k0[kDsMaxCycles];
-    __shared__ double s_part[512 / 32];
+    __shared__ double s_f[kDsMaxCycles];
+    __shared__ float* s_o[kDsMaxCycles];
+    __shared__ double s_part[kDsWarps];
 
     const int trial = blockIdx.y;
     const size_t N = job.lengths[trial];
-    const size_t seg0 = (size_t)blockIdx.x * kDsSeg;
+    const int seg = job.seg;
+    const size_t seg0 = (size_t)blockIdx.x * seg;
     if (seg0 >= N) return;
-    const float* z = job.in + job.in_off[trial];
-    const size_t L = std::min<size_t>(kDsStage, N - seg0);
+    const float* z = job.in + job.in_off[trial] + seg0;
+    const int L = (int)std::min<size_t>(kDsStage, N - seg0);
     const double mean = job.mean ? job.mean[trial] : 0.0;
     const double inv = job.norm ? job.norm[trial] : 1.0;
     const bool affine = job.mean != nullptr;
-    float* zout = job.norm_out ? job.norm_out + job.in_off[trial] : nullptr;
+    float* zout = job.norm_out ? job.norm_out + job.in_off[trial] + seg0 : nullptr;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
-    // stage (and optionally normalise) the segment + halo
-    for (size_t i = threadIdx.x; i < L; i += blockDim.x) {
-        float v = __ldg(z + seg0 + i);
-        if (affine) v = __double2float_rn(__ddiv_rn(__dsub_rn((double)v, mean), inv));
-        zs[i] = v;
-        if (zout && i < kDsSeg) zout[seg0 + i] = v;
-    }
-    __syncthreads();
-    // exclusive prefix in double: 512 threads x 16 contiguous elements
-    {
-        const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-        const int per = kDsStage / 512;
-        const int c0 = tid * per;
-        double local = 0.0;
-        for (int j = 0; j < per; ++j) {
-            const int i = c0 + j;
-            local += (i < (int)L) ? (double)zs[i] : 0.0;
-        }
-        double incl = local;
+    // Stage the segment + halo (and write the normalised copy if asked for). Warp w owns the
+    // staged samples [w * kDsPerWarp, (w + 1) * kDsPerWarp), lane-strided so every shared
+    // access is conflict-free.
+    double wsum = 0.0;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const double y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
+    for (int ch = 0; ch < kDsChunks; ++ch) {
+        const int i = warp * kDsPerWarp + ch * 32 + lane;
+        float x = 0.0f;
+        if (i < L) {
+            x = __ldg(z + i);
+            if (zout && i < seg)
+                zout[i] = __double2float_rn(__ddiv_rn(__dsub_rn((double)x, mean), inv));
         }
-        if (lane == 31) s_part[warp] = incl;
-        __syncthreads();
-        if (tid == 0) {
-            double run = 0.0;
-            for (int w = 0; w < 512 / 32; ++w) {
-                const double v = s_part[w];
-                s_part[w] = run;
-                run += v;
-            }
-        }
-        __syncthreads();
-        double ex = __shfl_up_sync(0xffffffffu, incl, 1);
-        if (lane == 0) ex = 0.0;
-        double run = s_part[warp] + ex;
-        for (int j = 0; j < per; ++j) {
-            const int i = c0 + j;
-            P[i] = run;
-            run += (i < (int)L) ? (double)zs[i] : 0.0;
-        }
-        if (tid == 511) P[kDsStage] = run;
+        zs[i] = x;
+        wsum += (double)x;
     }
-    // outputs per cycle whose imin lies in the segment
-    const size_t seg1 = std::min(N, seg0 + kDsSeg);
-    if (threadIdx.x < job.ncycles) {
-        const int c = threadIdx.x;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
+    if (lane == 0) s_part[warp] = wsum;
+
+    // per-cycle output ranges whose first sample imin = floor(k f) lies in the segment
+    const size_t seg1 = std::min(N, seg0 + (size_t)seg);
+    if (tid < job.ncycles) {
+        const int c = tid;
         const double f = job.f[c];
         const size_t n = downsampled_size(N, f);
         int cnt = 0;
@@ -402,36 +390,78 @@ __global__ void __launch_bounds__(512)
         }
         s_cnt[c] = cnt;
         s_k0[c] = k0;
+        s_f[c] = f;
+        s_o[c] = job.out + job.out_off[(size_t)trial * job.ncycles + c];
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+
+    // exclusive prefix in double: the warp's offset, then 32-sample shuffle scans
+    double carry = 0.0;
+    for (int w = 0; w < warp; ++w) carry += s_part[w];
+#pragma unroll
+    for (int ch = 0; ch < kDsChunks; ++ch) {
+        const double x = (double)zs[warp * kDsPerWarp + ch * 32 + lane];
+        double incl = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        double ex = __shfl_up_sync(0xffffffffu, incl, 1);
+        if (lane == 0) ex = 0.0;
+        P[warp * kDsPerWarp + ch * 32 + lane] = carry + ex;
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (tid == kDsThreads - 1) P[kDsStage] = carry;
+    if (tid == 0) {
         int run = 0;
         for (int c = 0; c < job.ncycles; ++c) {
-            const int v = s_cnt[c];
+            const int x = s_cnt[c];
             s_cnt[c] = run;
-            run += v;
+            run += x;
         }
         s_cnt[job.ncycles] = run;
     }
     __syncthreads();
-    const int total = s_cnt[job.ncycles];
-    for (int q = threadIdx.x; q < total; q += blockDim.x) {
+
+    // Outputs. The outputs of all cycles form one index range [0, total), taken by the warps
+    // in chunks of 32 consecutive indices (balanced across warps). The cycle of a chunk's first
+    // index comes from ballots over the cycle offsets; a lane steps forward across the cycle
+    // boundaries inside its chunk. Sample positions are made relative to seg0: start - seg0
+    // and end - seg0 are exact (seg0 is an integer at most start), so floor, weights and
+    // clamping give the same values as the absolute FP64 bounds of downsample.hpp:58-72.
+    const double seg0d = (double)seg0;
+    const double lastd = (double)(N - 1 - seg0);
+    const double rinv = 1.0 / inv;
+    const int nc = job.ncycles;
+    const int total = s_cnt[nc];
+    for (int base = warp * 32; base < total; base += kDsThreads) {
         int c = 0;
+        for (int c0 = 1; c0 < nc; c0 += 32) {
+            const int cc = c0 + lane;
+            c += __popc(__ballot_sync(0xffffffffu, cc < nc && s_cnt[cc] <= base));
+        }
+        const int q = base + lane;
+        if (q >= total) continue;
         while (s_cnt[c + 1] <= q) ++c;
-        const size_t k = s_k0[c] + (q - s_cnt[c]);
-        const double f = job.f[c];
+        const double f = s_f[c];
+        const size_t k = s_k0[c] + (size_t)(q - s_cnt[c]);
         const double start = (double)k * f;
         const double end = start + f;
-        const size_t imin = (size_t)floor(start);
-        const double fe = floor(end);
-        const size_t imax = (size_t)(fe < (double)N - 1.0 ? fe : (double)N - 1.0);
-        const float wmin = __double2float_rn((double)(imin + 1) - start);
-        const float wmax = __double2float_rn(end - (double)imax);
-        const size_t li = imin - seg0, ui = imax - seg0;
-        const double acc = (double)wmin * (double)zs[li] + (P[ui] - P[li + 1]) +
-                           (double)wmax * (double)zs[ui];
-        float* o = job.out + job.out_off[(size_t)trial * job.ncycles + c];
-        o[k] = __double2float_rn(acc);
+        const double sr = start - seg0d, er = end - seg0d;
+        // floors of values in [0, 2^13) as doubles; their integer values via the 2^52 + 2^51
+        // rounding constant (exact for integral doubles below 2^51)
+        const double fl = floor(sr);
+        const double fu = fmin(floor(er), lastd);
+        const int li = __double2loint(fl + 6755399441055744.0);
+        const int ui = __double2loint(fu + 6755399441055744.0);
+        const float wmin = __double2float_rn((fl + 1.0) - sr);
+        const float wmax = __double2float_rn(er - fu);
+        double acc = (double)wmin * (double)zs[li] + (P[ui] - P[li + 1]) +
+                     (double)wmax * (double)zs[ui];
+        if (affine)  // sum of (v - mean) / norm over the same weights, W = their total
+            acc = (acc - mean * ((double)wmin + (fu - fl - 1.0) + (double)wmax)) * rinv;
+        s_o[c][k] = __double2float_rn(acc);
     }
 }
 
@@ -445,6 +475,7 @@ __global__ void k_downsample_wide(DsJob job, int cycle)
     const float* z = job.in + job.in_off[trial];
     const double mean = job.mean ? job.mean[trial] : 0.0;
     const double inv = job.norm ? job.norm[trial] : 1.0;
+    const double rinv = 1.0 / inv;
     const bool affine = job.mean != nullptr;
     float* o = job.out + job.out_off[(size_t)trial * job.ncycles + cycle];
     const int lane = threadIdx.x & 31;
@@ -457,36 +488,39 @@ __global__ void k_downsample_wide(DsJob job, int cycle)
         const double fe = floor(end);
         const size_t imax = (size_t)(fe < (double)N - 1.0 ? fe : (double)N - 1.0);
         double acc = 0.0;
-        for (size_t i = imin + 1 + lane; i < imax; i += 32) {
-            float v = __ldg(z + i);
-            if (affine) v = __double2float_rn(__ddiv_rn(__dsub_rn((double)v, mean), inv));
-            acc += (double)v;
-        }
+        for (size_t i = imin + 1 + lane; i < imax; i += 32) acc += (double)__ldg(z + i);
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
         if (lane == 0) {
-            float a = __ldg(z + imin), bb = __ldg(z + imax);
-            if (affine) {
-                a = __double2float_rn(__ddiv_rn(__dsub_rn((double)a, mean), inv));
-                bb = __double2float_rn(__ddiv_rn(__dsub_rn((double)bb, mean), inv));
-            }
+            const float a = __ldg(z + imin), bb = __ldg(z + imax);
             const float wmin = __double2float_rn((double)(imin + 1) - start);
             const float wmax = __double2float_rn(end - (double)imax);
-            o[k] = __double2float_rn((double)wmin * a + acc + (double)wmax * bb);
+            double r = (double)wmin * a + acc + (double)wmax * bb;
+            if (affine)  // as in k_downsample_segments
+                r = (r - mean * ((double)wmin + (double)(imax - imin - 1) + (double)wmax)) * rinv;
+            o[k] = __double2float_rn(r);
         }
     }
 }
 
-int launch_downsample(const DsJob& job, int ntrials, size_t max_len, cudaStream_t st)
+int launch_downsample(const DsJob& job_in, int ntrials, size_t max_len, cudaStream_t st)
 {
+    DsJob job = job_in;
     bool any_seg = job.norm_out != nullptr;  // the segment pass also writes the normalised copy
-    for (int c = 0; c < job.ncycles; ++c) any_seg |= job.use_seg_host[c] != 0;
+    double fmax = 0.0;
+    for (int c = 0; c < job.ncycles; ++c) {
+        if (job.use_seg_host[c]) fmax = std::max(fmax, job.f_host[c]);
+        any_seg |= job.use_seg_host[c] != 0;
+    }
+    // halo >= f + 1 for every segment factor (ds_use_segments: f + 2 <= kDsHalo), in whole warps
+    const int halo = std::min(kDsHalo, ((int)ceil(fmax) + 2 + 31) & ~31);
+    job.seg = kDsStage - halo;
     if (any_seg) {
         const size_t smem = (kDsStage + 1) * sizeof(double) + kDsStage * sizeof(float);
         RT_TRY_CUDA(cudaFuncSetAttribute(k_downsample_segments,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        dim3 grid((unsigned)((max_len + kDsSeg - 1) / kDsSeg), (unsigned)ntrials);
-        k_downsample_segments<<<grid, 512, smem, st>>>(job);
+        dim3 grid((unsigned)((max_len + job.seg - 1) / job.seg), (unsigned)ntrials);
+        k_downsample_segments<<<grid, kDsThreads, smem, st>>>(job);
         RT_TRY_CUDA(cudaGetLastError());
     }
     for (int c = 0; c < job.ncycles; ++c) {

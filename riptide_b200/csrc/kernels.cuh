@@ -31,9 +31,8 @@ int launch_running_median(const float* x, const size_t* d_lengths, const size_t*
                           int ntrials, size_t max_len, int width, float* out, cudaStream_t st);
 
 // Downsampling of many series by many factors in one pass (device arrays).
-constexpr int kDsSeg = 4096;          // output ownership segment (input samples)
-constexpr int kDsHalo = 4096;         // staged samples beyond the segment
-constexpr int kDsStage = kDsSeg + kDsHalo;
+constexpr int kDsStage = 8192;        // input samples staged per CTA (segment + halo)
+constexpr int kDsHalo = 4096;         // largest halo: factors up to kDsHalo - 2
 constexpr int kDsMaxCycles = 256;
 
 struct DsJob {
@@ -48,7 +47,9 @@ struct DsJob {
     float* out;                 // packed outputs
     const size_t* out_off;      // [ntrials * ncycles]
     int ncycles;
+    int seg;                    // output ownership segment (input samples), set by the launcher
     // host copies for the launcher
+    const double* f_host;       // [ncycles]
     const int* use_seg_host;
     const int* skip_host;       // [ncycles] cycles with nothing to produce (f == 1)
 };
