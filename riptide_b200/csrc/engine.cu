@@ -361,8 +361,12 @@ __global__ void __launch_bounds__(kEngineThreads, 1) k_search_persistent(EngineA
                     cnt[2] += J.hi - J.lo;
                     cnt[3] += stage > 0;
                 }
+                // stage outputs other than the last are written by the root level itself
+                float* root_dst =
+                    last ? nullptr
+                         : root_rows_dst(T, b, slot + (size_t)(stage & 1) * A.slot_floats);
                 if (!run_job_levels(T, src, b, Lay.buf0, Lay.buf1, fstride, Lay.ops, staged_src,
-                                    &s_bar, &bar_phase)) {
+                                    &s_bar, &bar_phase, root_dst)) {
                     if (threadIdx.x == 0) atomicExch(A.error, RT_ETIMEOUT);
                 }
                 mark(kPhLevels);
@@ -372,9 +376,6 @@ __global__ void __launch_bounds__(kEngineThreads, 1) k_search_persistent(EngineA
                     else
                         final_stage_outputs<16>(T, X, A, S, Lay.buf0, Lay.buf1, fstride, cap_rows);
                     mark(kPhSnr);
-                } else {
-                    store_root_rows(T, Lay.buf0, fstride, b,
-                                    slot + (size_t)(stage & 1) * A.slot_floats);
                 }
             }
         }

@@ -262,15 +262,15 @@ __device__ __forceinline__ void level_rows_unrolled(const RowOp* ops, int nrows,
 // 32 consecutive words (mod b); the rolled row is read from p0 = (64 j + shift) mod b on.
 template <int NIT2>
 __device__ __forceinline__ void level_rows_pairs(const RowOp* ops, int nrows,
-                                                 const float* __restrict__ src,
+                                                 const float* __restrict__ src, int sstride,
                                                  float* __restrict__ dst, int stride, int b)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int r = warp; r < nrows; r += kWarps) {
         const RowOp op = ops[r];
         float* out = dst + (size_t)r * stride;
-        const float* H = src + (size_t)op.h * stride + lane;
-        const float* Tr = src + (size_t)op.t * stride;
+        const float* H = src + (size_t)op.h * sstride + lane;
+        const float* Tr = src + (size_t)op.t * sstride;
 #pragma unroll
         for (int j = 0; j < NIT2; ++j) {
             int p0 = op.shift + 64 * j;  // < b + 64 j: at most two wraps for NIT2 <= 9
@@ -319,10 +319,10 @@ __device__ __forceinline__ void level_rows(const RowOp* ops, int nrows, const fl
 {
     if (!kGlobal && halo_mode(b)) {
         switch ((b + 63) >> 6) {
-            case 4: level_rows_pairs<4>(ops, nrows, src, dst, stride, b); return;
-            case 5: level_rows_pairs<5>(ops, nrows, src, dst, stride, b); return;
-            case 8: level_rows_pairs<8>(ops, nrows, src, dst, stride, b); return;
-            default: level_rows_pairs<9>(ops, nrows, src, dst, stride, b); return;
+            case 4: level_rows_pairs<4>(ops, nrows, src, sstride, dst, stride, b); return;
+            case 5: level_rows_pairs<5>(ops, nrows, src, sstride, dst, stride, b); return;
+            case 8: level_rows_pairs<8>(ops, nrows, src, sstride, dst, stride, b); return;
+            default: level_rows_pairs<9>(ops, nrows, src, sstride, dst, stride, b); return;
         }
     }
     const int nit = (b + 31) >> 5;
@@ -336,10 +336,6 @@ __device__ __forceinline__ void level_rows(const RowOp* ops, int nrows, const fl
     }
 }
 
-// Runs all levels of the job. On return, the root rows [lo, hi) are in buf0 (stride
-// `stride`, row i of the buffer = root output row lo + i). `src` is the global source:
-// row j of it is at src + j * b (j in transform row indexing). `ops` has room for the
-// largest level.
 // Level computed from source rows staged in shared memory (packed, stride b): same loop as
 // the global level, plain loads.
 __device__ __forceinline__ void level_rows_staged(const RowOp* ops, int nrows, const float* src,
@@ -355,13 +351,17 @@ __device__ __forceinline__ void level_rows_staged(const RowOp* ops, int nrows, c
     }
 }
 
+// Runs all levels of the job. On return, the root rows [lo, hi) are in buf0 (stride
+// `stride`, row i of the buffer = root output row lo + i), or, if `root_dst` is given, at
+// root_dst + i * b in global memory. `src` is the global source: row j of it is at
+// src + j * b (j in transform row indexing). `ops` has room for the largest level.
 // `staged` (optional): the job's source rows already being copied into shared memory, as a
 // pointer such that global row j of the source is at staged + j * b; the copy completes on
 // phase `*phase` of `bar`. Returns false if that wait ran out.
 __device__ inline bool run_job_levels(const JobTree& T, const float* __restrict__ src, int b,
                                       float* buf0, float* buf1, int stride, RowOp* ops,
                                       const float* staged = nullptr, uint64_t* bar = nullptr,
-                                      uint32_t* phase = nullptr)
+                                      uint32_t* phase = nullptr, float* root_dst = nullptr)
 {
     build_all_ops(T, b, ops);
     cta_sync();
@@ -371,32 +371,30 @@ __device__ inline bool run_job_levels(const JobTree& T, const float* __restrict_
         *phase ^= 1u;
     }
     for (int d = T.depth; d >= 0; --d) {
-        float* dst = (d & 1) ? buf1 : buf0;
+        // the root level goes straight to global memory when the caller wants it there
+        const bool out_global = d == 0 && root_dst != nullptr;
+        float* dst = out_global ? root_dst : ((d & 1) ? buf1 : buf0);
+        const int dstride = out_global ? b : stride;
         const float* prev = (d & 1) ? buf0 : buf1;  // level d+1
         const RowOp* lops = ops + T.op_start[d];
         if (d == T.depth) {
             if (staged)
-                level_rows_staged(lops, T.level_rows[d], staged, dst, stride, b);
+                level_rows_staged(lops, T.level_rows[d], staged, dst, dstride, b);
             else
-                level_rows<true>(lops, T.level_rows[d], src, b, dst, stride, b);
+                level_rows<true>(lops, T.level_rows[d], src, b, dst, dstride, b);
         } else {
-            level_rows<false>(lops, T.level_rows[d], prev, stride, dst, stride, b);
+            level_rows<false>(lops, T.level_rows[d], prev, stride, dst, dstride, b);
         }
         cta_sync();
     }
     return ok;
 }
 
-// Writes the root rows held in buf0 to global rows (root_row0 + s) of `dst` (stride b).
-__device__ __forceinline__ void store_root_rows(const JobTree& T, const float* buf0, int stride,
-                                                int b, float* __restrict__ dst)
+// Global address of the root rows of a job in a stage output (stride b), for run_job_levels.
+__device__ __forceinline__ float* root_rows_dst(const JobTree& T, int b, float* dst)
 {
     const Node r = T.nodes[0];
-    const int nrows = r.hi - r.lo;
-    float* base = dst + (size_t)(r.row0 + r.lo) * b;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int row = warp; row < nrows; row += kWarps)
-        for (int c = lane; c < b; c += 32) base[(size_t)row * b + c] = buf0[(size_t)row * stride + c];
+    return dst + (size_t)(r.row0 + r.lo) * b;
 }
 
 // Shared-memory layout of a CTA running FFA jobs: [fixed part][ops][buf0][buf1].

@@ -159,8 +159,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (threadIdx.x == 0) atomicExch(err, RT_EINTERNAL);
         return;
     }
-    run_job_levels(T, src, b, L.buf0, L.buf1, stride, L.ops);
-    store_root_rows(T, L.buf0, stride, b, dst);
+    run_job_levels(T, src, b, L.buf0, L.buf1, stride, L.ops, nullptr, nullptr, nullptr,
+                   root_rows_dst(T, b, dst));
 }
 
 bool plan_stages(int m, int rows_out, int cap_rows, StagePlan* P)
