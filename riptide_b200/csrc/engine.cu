@@ -44,12 +44,14 @@ struct WorkItem {
     int stage_job;       // stage << 24 | job
 };
 
-// Shared-memory layout of the persistent kernel: job tree, S/N parameters, two level buffers.
+// Shared-memory layout of the persistent kernel: two job trees (static; one per item slot),
+// then (dynamic) S/N parameters and the two level buffers.
 constexpr size_t kEngineTreeBytes = (sizeof(JobTree) + 255) & ~size_t(255);
 constexpr size_t kEngineSnrBytes = (sizeof(SnrParams) + 255) & ~size_t(255);
+constexpr size_t kEngineDynBytes = kFfaSmemBytes - 2 * kEngineTreeBytes;
 RT_HD int engine_cap_rows(int b)
 {
-    return ffa_cap_rows_for(kFfaSmemBytes, kEngineTreeBytes + kEngineSnrBytes, b);
+    return ffa_cap_rows_for(kEngineDynBytes, kEngineSnrBytes, b);
 }
 
 constexpr int kSlots = 256;          // scratch slots for multi-stage transforms
@@ -197,7 +199,7 @@ __device__ void sched_decode(const EngineArgs& A, long long t, SchedItem& it)
 // have smaller tickets), so whichever scheduler holds it hands it over; every wait is bounded.
 constexpr int kParked = 4;
 
-__device__ void scheduler_warp(const EngineArgs& A, ItemSlot* slots)
+__device__ void scheduler_warp(const EngineArgs& A, ItemSlot* slots, JobTree* trees)
 {
     const int lane = threadIdx.x & 31;
     SchedItem parked[kParked];
@@ -264,6 +266,9 @@ __device__ void scheduler_warp(const EngineArgs& A, ItemSlot* slots)
         }
         __syncwarp();
         const bool stop = slots[s].ticket >= A.nitems || !slots[s].ok;
+        // the job tree of the item, built while the compute threads run the previous item
+        if (!stop && slots[s].J.hi > slots[s].J.lo)
+            build_job_tree_warp(trees[s], slots[s].J, slots[s].cap_rows);
         named_arrive(kBarFull + s, kEngineThreads);
         if (stop) break;
     }
@@ -274,17 +279,17 @@ __device__ void scheduler_warp(const EngineArgs& A, ItemSlot* slots)
 __global__ void __launch_bounds__(kEngineThreads, 1) k_search_persistent(EngineArgs A)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    JobTree& T = *reinterpret_cast<JobTree*>(smem);
-    SnrParams& S = *reinterpret_cast<SnrParams*>(smem + kEngineTreeBytes);
-    unsigned char* layout = smem + kEngineTreeBytes + kEngineSnrBytes;
+    SnrParams& S = *reinterpret_cast<SnrParams*>(smem);
+    unsigned char* layout = smem + kEngineSnrBytes;
     __shared__ ItemSlot slots[2];
+    __shared__ JobTree trees[2];
     __shared__ int s_b;
     __shared__ __align__(8) uint64_t s_bar;  // completion of the bulk copy of a job's rows
 
     if (threadIdx.x == 0) mbar_init(&s_bar, 1);
     __syncthreads();
     if (threadIdx.x >= kThreads) {
-        scheduler_warp(A, slots);
+        scheduler_warp(A, slots, trees);
         return;
     }
     uint32_t bar_phase = 0;
@@ -305,6 +310,7 @@ __global__ void __launch_bounds__(kEngineThreads, 1) k_search_persistent(EngineA
         named_sync(kBarFull + sl, kEngineThreads);
         mark(kPhWait);
         const ItemSlot& L = slots[sl];
+        const JobTree& T = trees[sl];
         if (L.ticket >= A.nitems || !L.ok) break;
         const XformRec X = L.X;
         const JobSpec J = L.J;
@@ -344,7 +350,6 @@ __global__ void __launch_bounds__(kEngineThreads, 1) k_search_persistent(EngineA
                 cta_sync();
                 staged_src = sbuf + s_delta - (ptrdiff_t)J.root_row0 * b;
             }
-            build_job_tree(T, J, cap_rows);
             failed = T.error != 0;
             if (failed) {
                 if (threadIdx.x == 0) atomicExch(A.error, RT_EINTERNAL);
@@ -969,7 +974,7 @@ static int engine_grid()
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_search_persistent, kEngineThreads,
-                                                  kFfaSmemBytes);
+                                                  kEngineDynBytes);
     return std::max(1, sms * std::max(per, 1));
 }
 
@@ -1079,9 +1084,9 @@ static int plan_run(SearchPlan& P, const float* data, float* normalised_out, dou
     A.phase_cycles = P.d_phase;
     RT_TRY_CUDA(cudaFuncSetAttribute(k_search_persistent,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)kFfaSmemBytes));
+                                     (int)kEngineDynBytes));
     if (A.nitems > 0) {
-        k_search_persistent<<<engine_grid(), kEngineThreads, kFfaSmemBytes, st>>>(A);
+        k_search_persistent<<<engine_grid(), kEngineThreads, kEngineDynBytes, st>>>(A);
         RT_TRY_CUDA(cudaGetLastError());
         launches += 1;
     }

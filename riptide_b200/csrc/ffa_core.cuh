@@ -149,6 +149,84 @@ __device__ inline void build_job_tree(JobTree& T, const JobSpec& J, int cap_rows
     cta_sync();
 }
 
+// The same job tree built by one warp (no CTA barrier), level by level: node i of level d is
+// the head (i even) or tail (i odd) child of node i >> 1 of level d - 1, which gives the
+// node list of build_job_tree.
+__device__ inline void build_job_tree_warp(JobTree& T, const JobSpec& J, int cap_rows)
+{
+    const int lane = threadIdx.x & 31;
+    const int G = J.G;
+    const bool bad = (G > kMaxJobDepth || (2 << G) - 1 > kMaxJobNodes);
+    if (lane == 0) {
+        T.depth = G;
+        T.error = bad ? 1 : 0;
+    }
+    if (bad) {
+        __syncwarp();
+        return;
+    }
+    if (lane == 0) {
+        Node nd;
+        nd.row0 = J.root_row0;
+        nd.rows = J.root_rows;
+        nd.lo = J.lo;
+        nd.hi = J.hi;
+        nd.off = 0;
+        T.nodes[0] = nd;
+    }
+    __syncwarp();
+    for (int d = 1; d <= G; ++d) {
+        const int base = (1 << d) - 1, pbase = (1 << (d - 1)) - 1;
+        for (int i = lane; i < (1 << d); i += 32) {
+            const Node p = T.nodes[pbase + (i >> 1)];
+            const int mh = p.rows >> 1;
+            const MergeCoef c = merge_coef(p.rows);
+            Node nd;
+            if (i & 1) {
+                nd.row0 = p.row0 + mh;
+                nd.rows = p.rows - mh;
+                nd.lo = merge_row(c.kt, p.lo);
+                nd.hi = merge_row(c.kt, p.hi - 1) + 1;
+            } else {
+                nd.row0 = p.row0;
+                nd.rows = mh;
+                nd.lo = merge_row(c.kh, p.lo);
+                nd.hi = merge_row(c.kh, p.hi - 1) + 1;
+            }
+            nd.off = 0;
+            T.nodes[base + i] = nd;
+        }
+        __syncwarp();
+    }
+    // per level: exclusive prefix of the row counts -> buffer offsets; then op_start
+    int acc = 0;
+    for (int d = 0; d <= G; ++d) {
+        const int n = 1 << d, base = n - 1;
+        int carry = 0;
+        for (int b0 = 0; b0 < n; b0 += 32) {
+            const int i = b0 + lane;
+            const int v = (i < n) ? (T.nodes[base + i].hi - T.nodes[base + i].lo) : 0;
+            int incl = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (i < n) T.nodes[base + i].off = carry + incl - v;
+            carry += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        if (lane == 0) {
+            T.level_start[d] = base;
+            T.level_rows[d] = carry;
+            T.op_start[d] = acc;
+            if (carry > cap_rows) T.error = 2;
+        }
+        acc += carry;
+    }
+    if (lane == 0) T.op_start[G + 1] = acc;
+    __syncwarp();
+}
+
 // Index of the node holding buffer row r at a level (nodes sorted by `off`).
 __device__ __forceinline__ int find_node(const Node* nodes, int n, int r)
 {
