@@ -121,11 +121,17 @@ __device__ __forceinline__ void window_max(const float* cr, int start, float (&m
 // the scratch rows C (stride cs), then take the width maxima from a register window. Only
 // warp-level synchronisation: a profile's TPR threads are lanes of one warp. Writes
 // out[r * out_stride + k]. `groups` profiles are processed at a time (C holds `groups` rows).
-template <int TPR, int SB>
-__device__ void snr_rows(const float* X, int xs, int nrows, int b, const SnrParams& S,
-                         float stdnoise, float* __restrict__ out, size_t out_stride, float* C,
-                         int cs, int groups)
+// Phases per thread of a TPR-thread profile for which the prefix passes are unrolled (the
+// thread's values held in registers): bins up to 264 with 8 threads, up to 544 with 16.
+template <int TPR>
+constexpr int snr_unrolled_phases() { return TPR == 8 ? 33 : 35; }
+
+template <int TPR, int SB, bool kUnrolled>
+__device__ void snr_rows_impl(const float* X, int xs, int nrows, int b, const SnrParams& S,
+                              float stdnoise, float* __restrict__ out, size_t out_stride,
+                              float* C, int cs, int groups)
 {
+    constexpr int PMAX = kUnrolled ? snr_unrolled_phases<TPR>() : 1;
     const int tid = threadIdx.x;
     const int g = tid / TPR, t = tid - g * TPR;
     const int ngroups = min(groups, kThreads / TPR);
@@ -136,9 +142,19 @@ __device__ void snr_rows(const float* X, int xs, int nrows, int b, const SnrPara
     float* cr = C + (size_t)g * cs;
     for (int r = g; r < nrows; r += ngroups) {
         const float* xr = X + (size_t)r * xs;
-        // prefix sums (kernels.hpp:73-101): exact sums (double-float), float stores
+        // prefix sums (kernels.hpp:73-101): exact sums (double-float), float stores. With at
+        // most PMAX phases per thread, the thread's values are loaded once into registers.
+        constexpr bool unrolled = kUnrolled;
+        float v[PMAX];
         float lh = 0.f, ll = 0.f;
-        for (int i = i0; i < i1; ++i) df_add(lh, ll, xr[i]);
+        if (unrolled) {
+#pragma unroll
+            for (int j = 0; j < PMAX; ++j) v[j] = (j < i1 - i0) ? xr[i0 + j] : 0.0f;
+#pragma unroll
+            for (int j = 0; j < PMAX; ++j) df_add(lh, ll, v[j]);
+        } else {
+            for (int i = i0; i < i1; ++i) df_add(lh, ll, xr[i]);
+        }
         float ih = lh, il = ll;  // inclusive scan over the TPR segments
 #pragma unroll
         for (int o = 1; o < TPR; o <<= 1) {
@@ -154,9 +170,17 @@ __device__ void snr_rows(const float* X, int xs, int nrows, int b, const SnrPara
         }
         float rh = __shfl_up_sync(gmask, ih, 1, TPR), rl = __shfl_up_sync(gmask, il, 1, TPR);
         if (t == 0) rh = rl = 0.f;
-        for (int i = i0; i < i1; ++i) {
-            df_add(rh, rl, xr[i]);
-            cr[i] = __fadd_rn(rh, rl);
+        if (unrolled) {
+#pragma unroll
+            for (int j = 0; j < PMAX; ++j) {
+                df_add(rh, rl, v[j]);  // adding the zero padding changes nothing stored
+                if (j < i1 - i0) cr[i0 + j] = __fadd_rn(rh, rl);
+            }
+        } else {
+            for (int i = i0; i < i1; ++i) {
+                df_add(rh, rl, xr[i]);
+                cr[i] = __fadd_rn(rh, rl);
+            }
         }
         const float th = __shfl_sync(gmask, ih, TPR - 1, TPR), tl = __shfl_sync(gmask, il, TPR - 1, TPR);
         const float sumx = __fadd_rn(th, tl);
@@ -202,6 +226,18 @@ __device__ void snr_rows(const float* X, int xs, int nrows, int b, const SnrPara
         }
         __syncwarp(gmask);  // cr is rewritten for the next profile
     }
+}
+
+template <int TPR, int SB>
+__device__ __forceinline__ void snr_rows(const float* X, int xs, int nrows, int b,
+                                         const SnrParams& S, float stdnoise,
+                                         float* __restrict__ out, size_t out_stride, float* C,
+                                         int cs, int groups)
+{
+    if ((((b + TPR - 1) / TPR) | 1) <= snr_unrolled_phases<TPR>())
+        snr_rows_impl<TPR, SB, true>(X, xs, nrows, b, S, stdnoise, out, out_stride, C, cs, groups);
+    else
+        snr_rows_impl<TPR, SB, false>(X, xs, nrows, b, S, stdnoise, out, out_stride, C, cs, groups);
 }
 
 // Row stride for prefix-sum rows: >= b + wmax and = TPR (mod 32), so that with an odd
