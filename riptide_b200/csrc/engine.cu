@@ -44,14 +44,14 @@ struct WorkItem {
     int stage_job;       // stage << 24 | job
 };
 
-// Shared-memory layout of the persistent kernel: two job trees (static; one per item slot),
-// then (dynamic) S/N parameters and the two level buffers.
+// Shared-memory layout of the persistent kernel: per item slot (static) a job tree and the
+// boxcar coefficients; the dynamic part holds the row operations and two level buffers.
 constexpr size_t kEngineTreeBytes = (sizeof(JobTree) + 255) & ~size_t(255);
 constexpr size_t kEngineSnrBytes = (sizeof(SnrParams) + 255) & ~size_t(255);
-constexpr size_t kEngineDynBytes = kFfaSmemBytes - 2 * kEngineTreeBytes;
+constexpr size_t kEngineDynBytes = kFfaSmemBytes - 2 * (kEngineTreeBytes + kEngineSnrBytes);
 RT_HD int engine_cap_rows(int b)
 {
-    return ffa_cap_rows_for(kEngineDynBytes, kEngineSnrBytes, b);
+    return ffa_cap_rows_for(kEngineDynBytes, 0, b);
 }
 
 constexpr int kSlots = 256;          // scratch slots for multi-stage transforms
@@ -109,7 +109,7 @@ __device__ bool wait_at_least(const int* p, int target, int* error)
 
 template <int TPR>
 __device__ void final_stage_outputs(const JobTree& T, const XformRec& X, const EngineArgs& A,
-                                    SnrParams& S, float* buf0, float* buf1, int fstride,
+                                    const SnrParams& S, float* buf0, float* buf1, int fstride,
                                     int cap_rows)
 {
     const Node r = T.nodes[0];
@@ -137,6 +137,7 @@ constexpr int kBarEmpty = 4;  // + slot
 struct ItemSlot {
     long long ticket;   // >= nitems: no more work
     int ok;             // 0: a wait failed, stop
+    int done_ok;        // set by the compute threads: 0 if the item failed
     int stage, last, cap_rows, jobs_of_stage;
     JobSpec J;
     XformRec X;
@@ -149,6 +150,37 @@ __device__ __forceinline__ void named_sync(int id, int n)
 __device__ __forceinline__ void named_arrive(int id, int n)
 {
     asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+
+// Per-slot count of compute warps done with the slot's item: each warp adds 1 with release
+// semantics at CTA scope; the scheduling warp reads it with acquire semantics.
+__device__ __forceinline__ void warp_done_release(unsigned* counter)
+{
+    asm volatile("red.release.cta.shared::cta.add.u32 [%0], 1;" ::"r"(smem_u32(counter))
+                 : "memory");
+}
+__device__ __forceinline__ unsigned warps_done_acquire(const unsigned* counter)
+{
+    unsigned v;
+    asm volatile("ld.acquire.cta.shared::cta.u32 %0, [%1];" : "=r"(v) : "r"(smem_u32(counter))
+                 : "memory");
+    return v;
+}
+
+// Completion of an item for the other CTAs: its stage counter and, after the last job of the
+// last stage, the release of the transform's scratch slot. Called by one thread after every
+// compute warp of the CTA has released the item (CTA scope); the fence makes their global
+// writes visible at GPU scope before the counters.
+__device__ __forceinline__ void signal_item_done(const EngineArgs& A, const ItemSlot& P)
+{
+    if (P.X.seq < 0 || !P.done_ok) return;
+    __threadfence();
+    int* d = A.done + (size_t)P.X.seq * kMaxStages + P.stage;
+    const int prev = atomicAdd(d, 1);
+    if (P.last && prev + 1 == P.jobs_of_stage) {
+        __threadfence();
+        atomicAdd(A.slot_release + (P.X.seq % kSlots), 1);
+    }
 }
 
 // Scheduler-side view of a claimed item: its slot contents and its dependency.
@@ -199,22 +231,35 @@ __device__ void sched_decode(const EngineArgs& A, long long t, SchedItem& it)
 // have smaller tickets), so whichever scheduler holds it hands it over; every wait is bounded.
 constexpr int kParked = 4;
 
-__device__ void scheduler_warp(const EngineArgs& A, ItemSlot* slots, JobTree* trees)
+__device__ void scheduler_warp(const EngineArgs& A, ItemSlot* slots, JobTree* trees,
+                               SnrParams* snr, unsigned* finished)
 {
     const int lane = threadIdx.x & 31;
     SchedItem parked[kParked];
     int nparked = 0;
     bool exhausted = false;
+    // items handed over whose completion is not signalled yet (lane 0): signalled as soon as
+    // every compute warp has released them, also while this warp waits for a dependency (an
+    // item it waits for may be the one running here)
+    bool pending[2] = {false, false};
+    auto try_signal = [&](int s) {
+        if (pending[s] && warps_done_acquire(finished + s) >= (unsigned)kWarps) {
+            signal_item_done(A, slots[s]);
+            pending[s] = false;
+        }
+    };
     int k = 0;
     for (;; ++k) {
         const int s = k & 1;
         if (k >= 2) named_sync(kBarEmpty + s, kEngineThreads);  // compute is done with item k-2
         if (lane == 0) {
+            try_signal(s);  // item k-2
             ItemSlot& L = slots[s];
             const long long w0 = clock64();
             bool chosen = false;
             unsigned ns = 32;
             for (long long spin = 0; !chosen; ++spin) {
+                try_signal(s ^ 1);  // item k-1, running
                 for (int i = 0; i < nparked && !chosen; ++i) {
                     if (sched_ready(parked[i])) {
                         L = parked[i].slot;
@@ -262,34 +307,43 @@ __device__ void scheduler_warp(const EngineArgs& A, ItemSlot* slots, JobTree* tr
                 if (ns < 1024) ns <<= 1;
             }
             if (A.phase_cycles) atomicAdd(A.phase_cycles + 7, (unsigned long long)(clock64() - w0));
+            L.done_ok = 1;
+            finished[s] = 0;
             __threadfence_block();
         }
         __syncwarp();
         const bool stop = slots[s].ticket >= A.nitems || !slots[s].ok;
-        // the job tree of the item, built while the compute threads run the previous item
-        if (!stop && slots[s].J.hi > slots[s].J.lo)
+        // the job tree and boxcar coefficients of the item, prepared while the compute threads
+        // run the previous item
+        if (!stop && slots[s].J.hi > slots[s].J.lo) {
             build_job_tree_warp(trees[s], slots[s].J, slots[s].cap_rows);
+            if (slots[s].last) snr_params_fill_warp(snr[s], A.widths, A.nw, A.nfast, slots[s].X.b);
+        }
         named_arrive(kBarFull + s, kEngineThreads);
         if (stop) break;
+        if (lane == 0) pending[s] = true;
     }
     // the compute threads still hand back the slot of item k-1
-    if (k >= 1) named_sync(kBarEmpty + ((k - 1) & 1), kEngineThreads);
+    if (k >= 1) {
+        named_sync(kBarEmpty + ((k - 1) & 1), kEngineThreads);
+        if (lane == 0) try_signal((k - 1) & 1);
+    }
 }
 
 __global__ void __launch_bounds__(kEngineThreads, 1) k_search_persistent(EngineArgs A)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    SnrParams& S = *reinterpret_cast<SnrParams*>(smem);
-    unsigned char* layout = smem + kEngineSnrBytes;
+    unsigned char* layout = smem;
     __shared__ ItemSlot slots[2];
     __shared__ JobTree trees[2];
-    __shared__ int s_b;
+    __shared__ SnrParams snr[2];
+    __shared__ unsigned finished[2];
     __shared__ __align__(8) uint64_t s_bar;  // completion of the bulk copy of a job's rows
 
     if (threadIdx.x == 0) mbar_init(&s_bar, 1);
     __syncthreads();
     if (threadIdx.x >= kThreads) {
-        scheduler_warp(A, slots, trees);
+        scheduler_warp(A, slots, trees, snr, finished);
         return;
     }
     uint32_t bar_phase = 0;
@@ -304,19 +358,18 @@ __global__ void __launch_bounds__(kEngineThreads, 1) k_search_persistent(EngineA
             tprev = t;
         }
     };
-    if (threadIdx.x == 0) s_b = -1;
     for (int k = 0;; ++k) {
         const int sl = k & 1;
         named_sync(kBarFull + sl, kEngineThreads);
         mark(kPhWait);
         const ItemSlot& L = slots[sl];
         const JobTree& T = trees[sl];
+        const SnrParams& S = snr[sl];
         if (L.ticket >= A.nitems || !L.ok) break;
         const XformRec X = L.X;
         const JobSpec J = L.J;
         const int stage = L.stage;
         const bool last = L.last != 0;
-        const int jobs_of_stage = L.jobs_of_stage;
         const int b = X.b;
         const int fstride = ffa_stride(b);
         const int cap_rows = L.cap_rows;
@@ -324,11 +377,6 @@ __global__ void __launch_bounds__(kEngineThreads, 1) k_search_persistent(EngineA
         float* slot = (X.seq >= 0) ? A.scratch + (size_t)(X.seq % kSlots) * 2 * A.slot_floats
                                    : nullptr;
         mark(6);
-        if (b != s_b) {  // boxcar coefficients depend on b
-            snr_params_fill(S, A.widths, A.nw, A.nfast, b);
-            if (threadIdx.x == 0) s_b = b;
-            cta_sync();
-        }
         mark(kPhFetch);
         bool failed = false;
         if (J.hi > J.lo) {
@@ -384,16 +432,11 @@ __global__ void __launch_bounds__(kEngineThreads, 1) k_search_persistent(EngineA
                 }
             }
         }
-        cta_sync();
-        if (threadIdx.x == 0 && X.seq >= 0 && !failed) {
-            __threadfence();
-            int* d = A.done + (size_t)X.seq * kMaxStages + stage;
-            const int prev = atomicAdd(d, 1);
-            if (last && prev + 1 == jobs_of_stage) {
-                __threadfence();
-                atomicAdd(A.slot_release + (X.seq % kSlots), 1);
-            }
-        }
+        // hand the item back: the scheduling warp signals its completion to the other CTAs
+        // once every compute warp has released it
+        if (threadIdx.x == 0 && failed) slots[sl].done_ok = 0;
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) warp_done_release(finished + sl);
         mark(kPhStore);
         named_arrive(kBarEmpty + sl, kEngineThreads);
     }

@@ -68,6 +68,25 @@ __device__ inline void snr_params_fill(SnrParams& S, const int* widths, int nw, 
     cta_sync();
 }
 
+// The same parameters filled by one warp (no CTA barrier).
+__device__ inline void snr_params_fill_warp(SnrParams& S, const int* widths, int nw, int nfast,
+                                            int b)
+{
+    const int lane = threadIdx.x & 31;
+    if (lane == 0) {
+        S.nw = nw;
+        S.nfast = nfast;
+        int wm = 0;
+        for (int k = 0; k < nw; ++k) wm = widths[k] > wm ? widths[k] : wm;
+        S.wmax = wm;
+    }
+    for (int k = lane; k < nw; k += 32) {
+        S.w[k] = widths[k];
+        boxcar_coefs(b, widths[k], &S.hb[k], &S.beta[k]);
+    }
+    __syncwarp();
+}
+
 // Double-float accumulation (Knuth's TwoSum): (hi, lo) holds a sum exactly while it needs no
 // more than about 48 significant bits -- the float32 counterpart of the reference's double
 // accumulator (kernels.hpp:75-83), which is exact up to 53 bits. round(hi + lo) is then the
