@@ -316,7 +316,7 @@ __device__ void scheduler_warp(const EngineArgs& A, ItemSlot* slots, JobTree* tr
         // the job tree and boxcar coefficients of the item, prepared while the compute threads
         // run the previous item
         if (!stop && slots[s].J.hi > slots[s].J.lo) {
-            build_job_tree_warp(trees[s], slots[s].J, slots[s].cap_rows);
+            build_job_tree_warp(trees[s], slots[s].J, slots[s].cap_rows, slots[s].stage > 0);
             if (slots[s].last) snr_params_fill_warp(snr[s], A.widths, A.nw, A.nfast, slots[s].X.b);
         }
         named_arrive(kBarFull + s, kEngineThreads);
@@ -383,20 +383,30 @@ __global__ void __launch_bounds__(kEngineThreads, 1) k_search_persistent(EngineA
             const float* src =
                 (stage == 0) ? (X.src_norm ? A.norm : A.ds) + X.src_off
                              : slot + (size_t)((stage - 1) & 1) * A.slot_floats;
-            // stage-0 jobs (whole subtrees) read one contiguous block of rows of the
-            // downsampled arena (padded): copy it into the buffer level G reads from, in the
-            // background of the job-tree build
-            const bool staged = stage == 0 && !X.src_norm && J.root_rows <= cap_rows &&
-                                (size_t)J.root_rows * b + 8 <= (size_t)cap_rows * fstride;
-            const float* staged_src = nullptr;
-            if (staged) {
-                float* sbuf = (J.G & 1) ? Lay.buf0 : Lay.buf1;
+            LevelIO io;
+            io.src = src;
+            io.src_stride = (stage == 0) ? b : fstride;  // stage outputs: level stride
+            io.bar = &s_bar;
+            io.phase = &bar_phase;
+            // Level G's source rows are copied (bulk copies) into the level buffer that level G
+            // does not write, in the background of the row-operation build: for stage-0 jobs
+            // (whole subtrees) one contiguous block of the downsampled arena (padded); for
+            // later stages the blocks of the previous stage's output that the cone needs.
+            float* sbuf = (J.G & 1) ? Lay.buf0 : Lay.buf1;
+            const bool staged0 = stage == 0 && !X.src_norm && J.root_rows <= cap_rows &&
+                                 (size_t)J.root_rows * b + 8 <= (size_t)cap_rows * fstride;
+            const bool staged = staged0 || (stage > 0 && T.pstaged && !T.error);
+            if (staged0) {
                 __shared__ int s_delta;
                 if (threadIdx.x == 0)
                     s_delta = stage_rows_async(sbuf, src + (size_t)J.root_row0 * b,
                                                (size_t)J.root_rows * b, &s_bar);
                 cta_sync();
-                staged_src = sbuf + s_delta - (ptrdiff_t)J.root_row0 * b;
+                io.staged = sbuf + s_delta - (ptrdiff_t)J.root_row0 * b;
+            } else if (staged) {
+                if (threadIdx.x < 32) stage_source_rows_async(T, src, fstride, sbuf, &s_bar);
+                io.staged = sbuf;
+                io.staged_rows = true;
             }
             failed = T.error != 0;
             if (failed) {
@@ -415,11 +425,12 @@ __global__ void __launch_bounds__(kEngineThreads, 1) k_search_persistent(EngineA
                     cnt[3] += stage > 0;
                 }
                 // stage outputs other than the last are written by the root level itself
-                float* root_dst =
-                    last ? nullptr
-                         : root_rows_dst(T, b, slot + (size_t)(stage & 1) * A.slot_floats);
-                if (!run_job_levels(T, src, b, Lay.buf0, Lay.buf1, fstride, Lay.ops, staged_src,
-                                    &s_bar, &bar_phase, root_dst)) {
+                if (!last) {
+                    io.root_dst =
+                        root_rows_dst(T, fstride, slot + (size_t)(stage & 1) * A.slot_floats);
+                    io.root_stride = fstride;
+                }
+                if (!run_job_levels(T, b, Lay.buf0, Lay.buf1, fstride, Lay.ops, io)) {
                     if (threadIdx.x == 0) atomicExch(A.error, RT_ETIMEOUT);
                 }
                 mark(kPhLevels);
@@ -900,7 +911,8 @@ static int plan_build(SearchPlan& P)
                 const int xi = (int)P.xforms.size();
                 if (multi) {
                     X.seq = P.nseq++;
-                    P.slot_floats = std::max(P.slot_floats, rows * b);
+                    // stage outputs use the level stride (16-byte aligned rows)
+                    P.slot_floats = std::max(P.slot_floats, rows * (size_t)ffa_stride((int)b));
                     seq_xform.push_back(xi);
                     seq_pending.emplace_back();
                     seq_has_pending.push_back(0);

@@ -50,6 +50,12 @@ struct JobTree {
     int op_start[kMaxJobDepth + 2];     // first row operation of each level
     int depth;                          // G: nodes at this level read the global source
     int error;                          // nonzero if the job does not fit
+    // Source rows of level G staged in shared memory (jobs of later stages, whose source is
+    // the previous stage's output with 16-byte aligned rows): node i of level G reads its
+    // head child's rows [hlo, hhi) from staged rows src_off[i] + (h - hlo) and its tail
+    // child's rows [tlo, thi) right after them. pstaged = 0: level G reads global rows.
+    int pstaged;
+    int src_off[(kMaxJobNodes + 1) / 2 + 1];
 };
 
 // Description of one job, produced by the planners (host).
@@ -79,6 +85,7 @@ __device__ inline void build_job_tree(JobTree& T, const JobSpec& J, int cap_rows
     if (tid == 0) {
         T.depth = G;
         T.error = bad ? 1 : 0;
+        T.pstaged = 0;
     }
     if (bad) {
         cta_sync();
@@ -152,7 +159,10 @@ __device__ inline void build_job_tree(JobTree& T, const JobSpec& J, int cap_rows
 // The same job tree built by one warp (no CTA barrier), level by level: node i of level d is
 // the head (i even) or tail (i odd) child of node i >> 1 of level d - 1, which gives the
 // node list of build_job_tree.
-__device__ inline void build_job_tree_warp(JobTree& T, const JobSpec& J, int cap_rows)
+// With stage_source, also lays out the level-G source rows for staging (src_off, pstaged):
+// set when every level-G node has two children and the rows fit the level buffer.
+__device__ inline void build_job_tree_warp(JobTree& T, const JobSpec& J, int cap_rows,
+                                           bool stage_source = false)
 {
     const int lane = threadIdx.x & 31;
     const int G = J.G;
@@ -160,6 +170,7 @@ __device__ inline void build_job_tree_warp(JobTree& T, const JobSpec& J, int cap
     if (lane == 0) {
         T.depth = G;
         T.error = bad ? 1 : 0;
+        T.pstaged = 0;
     }
     if (bad) {
         __syncwarp();
@@ -224,6 +235,39 @@ __device__ inline void build_job_tree_warp(JobTree& T, const JobSpec& J, int cap
         acc += carry;
     }
     if (lane == 0) T.op_start[G + 1] = acc;
+    if (stage_source) {
+        // rows each level-G node needs from its two children, as consecutive staged blocks
+        const int n = 1 << G, base = n - 1;
+        int carry = 0;
+        bool two = true;
+        for (int b0 = 0; b0 < n; b0 += 32) {
+            const int i = b0 + lane;
+            int v = 0;
+            if (i < n) {
+                const Node nd = T.nodes[base + i];
+                if (nd.rows < 2) {
+                    two = false;
+                } else if (nd.hi > nd.lo) {
+                    const MergeCoef c = merge_coef(nd.rows);
+                    v = (merge_row(c.kh, nd.hi - 1) + 1 - merge_row(c.kh, nd.lo)) +
+                        (merge_row(c.kt, nd.hi - 1) + 1 - merge_row(c.kt, nd.lo));
+                }
+            }
+            int incl = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (i < n) T.src_off[i] = carry + incl - v;
+            carry += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        two = __all_sync(0xffffffffu, two);
+        if (lane == 0) {
+            T.src_off[n] = carry;
+            T.pstaged = (two && carry <= cap_rows) ? 1 : 0;
+        }
+    }
     __syncwarp();
 }
 
@@ -269,7 +313,12 @@ __device__ __forceinline__ RowOp make_row_op(const JobTree& T, int d, int r, int
         const MergeCoef c = merge_coef(nd.rows);
         const int h = merge_row(c.kh, s), t = merge_row(c.kt, s);
         op.shift = (s - t) % b;
-        if (d == T.depth) {
+        if (d == T.depth && T.pstaged) {
+            const int hlo = merge_row(c.kh, nd.lo);
+            const int hn = merge_row(c.kh, nd.hi - 1) + 1 - hlo;
+            op.h = T.src_off[i] + (h - hlo);
+            op.t = T.src_off[i] + hn + (t - merge_row(c.kt, nd.lo));
+        } else if (d == T.depth) {
             op.h = nd.row0 + h;
             op.t = nd.row0 + (nd.rows >> 1) + t;
         } else {
@@ -429,50 +478,99 @@ __device__ __forceinline__ void level_rows_staged(const RowOp* ops, int nrows, c
     }
 }
 
+// Where a job's levels read and write outside the two level buffers.
+struct LevelIO {
+    const float* src = nullptr;     // global source: row j at src + j * src_stride
+    int src_stride = 0;
+    const float* staged = nullptr;  // optional source rows being copied into shared memory
+    bool staged_rows = false;       // staged: true = rows of the layout in JobTree::src_off
+                                    // (stride = the level stride); false = global row j at
+                                    // staged + j * b
+    uint64_t* bar = nullptr;        // the copy completes on phase *phase of bar
+    uint32_t* phase = nullptr;
+    float* root_dst = nullptr;      // optional: root rows go to root_dst + i * root_stride
+    int root_stride = 0;
+};
+
 // Runs all levels of the job. On return, the root rows [lo, hi) are in buf0 (stride
-// `stride`, row i of the buffer = root output row lo + i), or, if `root_dst` is given, at
-// root_dst + i * b in global memory. `src` is the global source: row j of it is at
-// src + j * b (j in transform row indexing). `ops` has room for the largest level.
-// `staged` (optional): the job's source rows already being copied into shared memory, as a
-// pointer such that global row j of the source is at staged + j * b; the copy completes on
-// phase `*phase` of `bar`. Returns false if that wait ran out.
-__device__ inline bool run_job_levels(const JobTree& T, const float* __restrict__ src, int b,
-                                      float* buf0, float* buf1, int stride, RowOp* ops,
-                                      const float* staged = nullptr, uint64_t* bar = nullptr,
-                                      uint32_t* phase = nullptr, float* root_dst = nullptr)
+// `stride`, row i of the buffer = root output row lo + i), or in global memory if
+// io.root_dst is given. `ops` has room for the largest level. Returns false if the wait for
+// staged rows ran out.
+__device__ inline bool run_job_levels(const JobTree& T, int b, float* buf0, float* buf1,
+                                      int stride, RowOp* ops, const LevelIO& io)
 {
     build_all_ops(T, b, ops);
     cta_sync();
     bool ok = true;
-    if (staged) {
-        ok = mbar_wait(bar, *phase);
-        *phase ^= 1u;
+    if (io.staged) {
+        ok = mbar_wait(io.bar, *io.phase);
+        *io.phase ^= 1u;
     }
     for (int d = T.depth; d >= 0; --d) {
         // the root level goes straight to global memory when the caller wants it there
-        const bool out_global = d == 0 && root_dst != nullptr;
-        float* dst = out_global ? root_dst : ((d & 1) ? buf1 : buf0);
-        const int dstride = out_global ? b : stride;
-        const float* prev = (d & 1) ? buf0 : buf1;  // level d+1
+        const bool out_global = d == 0 && io.root_dst != nullptr;
+        float* dst = out_global ? io.root_dst : ((d & 1) ? buf1 : buf0);
+        const int dstride = out_global ? io.root_stride : stride;
         const RowOp* lops = ops + T.op_start[d];
-        if (d == T.depth) {
-            if (staged)
-                level_rows_staged(lops, T.level_rows[d], staged, dst, dstride, b);
-            else
-                level_rows<true>(lops, T.level_rows[d], src, b, dst, dstride, b);
+        // one call site per level loop kind (the loops are large once unrolled)
+        const bool first = d == T.depth;
+        if (first && !io.staged) {
+            level_rows<true>(lops, T.level_rows[d], io.src, io.src_stride, dst, dstride, b);
+        } else if (first && !io.staged_rows) {
+            level_rows_staged(lops, T.level_rows[d], io.staged, dst, dstride, b);
         } else {
-            level_rows<false>(lops, T.level_rows[d], prev, stride, dst, dstride, b);
+            // shared-memory source: level d + 1, or the staged rows of level G's children
+            const float* from = first ? io.staged : ((d & 1) ? buf0 : buf1);
+            level_rows<false>(lops, T.level_rows[d], from, stride, dst, dstride, b);
         }
         cta_sync();
     }
     return ok;
 }
 
-// Global address of the root rows of a job in a stage output (stride b), for run_job_levels.
-__device__ __forceinline__ float* root_rows_dst(const JobTree& T, int b, float* dst)
+// Global address of the root rows of a job in a stage output (row stride `rstride`).
+__device__ __forceinline__ float* root_rows_dst(const JobTree& T, int rstride, float* dst)
 {
     const Node r = T.nodes[0];
-    return dst + (size_t)(r.row0 + r.lo) * b;
+    return dst + (size_t)(r.row0 + r.lo) * rstride;
+}
+
+// Issued by one warp: bulk copies of the level-G source rows of a job laid out by
+// build_job_tree_warp (pstaged), from a global source of 16-byte aligned rows of `stride`
+// floats into `sbuf` (same stride), completing on `bar` (one arrival with the byte count).
+__device__ inline void stage_source_rows_async(const JobTree& T, const float* src, int stride,
+                                               float* sbuf, uint64_t* bar)
+{
+    const int lane = threadIdx.x & 31;
+    const int G = T.depth, n = 1 << G, base = n - 1;
+    const size_t row_bytes = (size_t)stride * sizeof(float);
+    // the source was written by other CTAs (generic proxy) before they signalled it
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (lane == 0) mbar_arrive_expect_tx(bar, (uint32_t)(T.src_off[n] * row_bytes));
+    __syncwarp();
+    constexpr uint32_t kChunk = 32768;
+    for (int i = lane; i < n; i += 32) {
+        const Node nd = T.nodes[base + i];
+        if (nd.hi <= nd.lo) continue;
+        const MergeCoef c = merge_coef(nd.rows);
+        const int hlo = merge_row(c.kh, nd.lo), hn = merge_row(c.kh, nd.hi - 1) + 1 - hlo;
+        const int tlo = merge_row(c.kt, nd.lo), tn = merge_row(c.kt, nd.hi - 1) + 1 - tlo;
+        const int r0[2] = {nd.row0 + hlo, nd.row0 + (nd.rows >> 1) + tlo};
+        const int cnt[2] = {hn, tn};
+        int off = T.src_off[i];
+        for (int h = 0; h < 2; ++h) {
+            const unsigned char* from =
+                reinterpret_cast<const unsigned char*>(src + (size_t)r0[h] * stride);
+            unsigned char* to = reinterpret_cast<unsigned char*>(sbuf + (size_t)off * stride);
+            const size_t bytes = (size_t)cnt[h] * row_bytes;
+            for (size_t o = 0; o < bytes; o += kChunk) {
+                const uint32_t nb = (uint32_t)(bytes - o < kChunk ? bytes - o : kChunk);
+                bulk_g2s(to + o, from + o, nb, bar);
+            }
+            off += cnt[h];
+        }
+    }
 }
 
 // Shared-memory layout of a CTA running FFA jobs: [fixed part][ops][buf0][buf1].

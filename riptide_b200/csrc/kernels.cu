@@ -159,8 +159,12 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (threadIdx.x == 0) atomicExch(err, RT_EINTERNAL);
         return;
     }
-    run_job_levels(T, src, b, L.buf0, L.buf1, stride, L.ops, nullptr, nullptr, nullptr,
-                   root_rows_dst(T, b, dst));
+    LevelIO io;
+    io.src = src;
+    io.src_stride = b;
+    io.root_dst = root_rows_dst(T, b, dst);
+    io.root_stride = b;
+    run_job_levels(T, b, L.buf0, L.buf1, stride, L.ops, io);
 }
 
 bool plan_stages(int m, int rows_out, int cap_rows, StagePlan* P)
