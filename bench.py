@@ -153,36 +153,22 @@ def traffic_per_trial():
 
 
 def dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
+    """One process per GPU (torchrun environment); NCCL process group for N > 1."""
+    from riptide_b200 import distributed as D
 
-        import torch
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    return world, rank, local
+    return D.init_from_env(backend="nccl", timeout_s=600)
 
 
 def max_over_ranks(v, world):
-    if world == 1:
-        return v
-    import torch
-    import torch.distributed as dist
+    from riptide_b200 import distributed as D
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return D.max_over_ranks(v, world)
 
 
 def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
+    from riptide_b200 import distributed as D
 
-        dist.barrier()
+    D.barrier(world)
 
 
 # --------------------------------------------------------------------------------------
