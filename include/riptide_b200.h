@@ -168,6 +168,12 @@ int rt_search_run(rt_search_plan* plan, const float* d_data, float* d_normalised
                   double* d_periods, uint32_t* d_foldbins, float* d_snrs, void* stream);
 /* Synchronises `stream` and reports a device-side failure of the last run. */
 int rt_search_check(rt_search_plan* plan, void* stream);
+/* Replays every later run as one CUDA graph (the run's launches and memsets, captured on
+ * the first run with these device pointers, and again when the pointers change); the graph
+ * is launched on the run's stream. Runs with stage timing enabled are not replayed. */
+int rt_search_set_graph(rt_search_plan* plan, int enable);
+/* Number of graph captures made so far (for checking that replays reuse the graph). */
+int rt_search_graph_captures(const rt_search_plan* plan, int* h_count);
 /* Per-stage CUDA-event timing of rt_search_run (events recorded on the run's stream). */
 int rt_search_set_timing(rt_search_plan* plan, int enable);
 /* Milliseconds of the last timed run: h_ms[0] deredden + normalise statistics,

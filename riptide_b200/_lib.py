@@ -51,6 +51,8 @@ SIGNATURES = {
     "rt_search_phase_cycles": (ctypes.c_int, [_vp, _u64p, ctypes.c_int]),
     "rt_search_plan_destroy": (None, [_vp]),
     "rt_search_plan_prepare": (ctypes.c_int, [_vp]),
+    "rt_search_set_graph": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "rt_search_graph_captures": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
     "rt_search_pipeline_create": (ctypes.c_int, [_u64p, _sz, _vp, _u64p, _sz, _sz, ctypes.POINTER(_vp)]),
     "rt_search_pipeline_rows": (ctypes.c_int, [_vp, _u64p]),
     "rt_search_pipeline_chunks": (ctypes.c_int, [_vp, ctypes.POINTER(_sz)]),

@@ -113,6 +113,16 @@ class BatchedSearch(object):
             return out, zs
         return out
 
+    def enable_graph(self, enable=True):
+        """Replay each run as one CUDA graph (captured again when the tensors change)."""
+        _lib.check(_lib.load().rt_search_set_graph(self._plan, int(bool(enable))))
+
+    @property
+    def graph_captures(self):
+        n = ctypes.c_int(0)
+        _lib.check(_lib.load().rt_search_graph_captures(self._plan, ctypes.byref(n)))
+        return int(n.value)
+
     def enable_timing(self, enable=True):
         """Record CUDA events around the stages of every run (see last_timing)."""
         _lib.check(_lib.load().rt_search_set_timing(self._plan, int(bool(enable))))

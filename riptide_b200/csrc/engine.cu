@@ -781,6 +781,13 @@ struct SearchPlan {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     unsigned long long* d_phase = nullptr;  // in-kernel phase profile (optional)
     int launches_last_run = 0;
+    // replay of the whole run as one CUDA graph (optional); the graph is keyed on the
+    // run's device pointers and captured again when they change
+    bool use_graph = false;
+    cudaGraphExec_t gexec = nullptr;
+    cudaStream_t cap_stream = nullptr;
+    const void* gkey[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    int graph_captures = 0;
 };
 
 static int plan_cycles(SearchPlan& P)
@@ -1243,12 +1250,72 @@ extern "C" int rt_search_plan_stats(const rt_search_plan* plan, rt_search_plan_s
     return RT_OK;
 }
 
+// Graph replay of plan_run: captured on the plan's own stream (the legacy default stream
+// cannot be captured), launched on the caller's.
+static int plan_run_graph(SearchPlan& P, const float* data, float* normalised_out,
+                          double* periods, uint32_t* foldbins, float* snrs, cudaStream_t st)
+{
+    const void* key[5] = {data, normalised_out, periods, foldbins, snrs};
+    bool same = P.gexec != nullptr;
+    for (int i = 0; i < 5; ++i) same = same && key[i] == P.gkey[i];
+    if (!same) {
+        RT_TRY(plan_prepare_device(P));  // allocations happen outside the capture
+        if (!P.cap_stream)
+            RT_TRY_CUDA(cudaStreamCreateWithFlags(&P.cap_stream, cudaStreamNonBlocking));
+        if (P.gexec) {
+            cudaGraphExecDestroy(P.gexec);
+            P.gexec = nullptr;
+        }
+        RT_TRY_CUDA(cudaStreamBeginCapture(P.cap_stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = plan_run(P, data, normalised_out, periods, foldbins, snrs, P.cap_stream);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(P.cap_stream, &g);
+        if (rc != RT_OK) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (ec != cudaSuccess) return check_cuda(ec, "cudaStreamEndCapture");
+        const cudaError_t ei = cudaGraphInstantiate(&P.gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+            P.gexec = nullptr;
+            return check_cuda(ei, "cudaGraphInstantiate");
+        }
+        for (int i = 0; i < 5; ++i) P.gkey[i] = key[i];
+        ++P.graph_captures;
+    }
+    RT_TRY_CUDA(cudaGraphLaunch(P.gexec, st));
+    return RT_OK;
+}
+
 extern "C" int rt_search_run(rt_search_plan* plan, const float* data, float* normalised_out,
                              double* periods, uint32_t* foldbins, float* snrs, void* stream)
 {
     if (!plan || !data || !periods || !foldbins || !snrs) return set_error(RT_EINVAL, "null argument");
     cudaStream_t st = (cudaStream_t)stream;
-    return plan_run(plan->p, data, normalised_out, periods, foldbins, snrs, st);
+    SearchPlan& P = plan->p;
+    if (P.use_graph && !P.timing)
+        return plan_run_graph(P, data, normalised_out, periods, foldbins, snrs, st);
+    return plan_run(P, data, normalised_out, periods, foldbins, snrs, st);
+}
+
+extern "C" int rt_search_set_graph(rt_search_plan* plan, int enable)
+{
+    if (!plan) return set_error(RT_EINVAL, "null argument");
+    SearchPlan& P = plan->p;
+    P.use_graph = enable != 0;
+    if (!P.use_graph && P.gexec) {
+        RT_TRY_CUDA(cudaGraphExecDestroy(P.gexec));
+        P.gexec = nullptr;
+    }
+    return RT_OK;
+}
+
+extern "C" int rt_search_graph_captures(const rt_search_plan* plan, int* h_count)
+{
+    if (!plan || !h_count) return set_error(RT_EINVAL, "null argument");
+    *h_count = plan->p.graph_captures;
+    return RT_OK;
 }
 
 extern "C" int rt_search_plan_prepare(rt_search_plan* plan)
@@ -1315,6 +1382,8 @@ extern "C" void rt_search_plan_destroy(rt_search_plan* plan)
     if (!plan) return;
     cudaDeviceSynchronize();
     if (plan->p.d_phase) cudaFree(plan->p.d_phase);
+    if (plan->p.gexec) cudaGraphExecDestroy(plan->p.gexec);
+    if (plan->p.cap_stream) cudaStreamDestroy(plan->p.cap_stream);
     for (int i = 0; i < 4; ++i)
         if (plan->p.ev[i]) cudaEventDestroy(plan->p.ev[i]);
     plan_free_device(plan->p);

@@ -93,6 +93,7 @@ static int pipeline_build(rt_search_pipeline* P, const uint64_t* lengths, size_t
         cc.nr = r[c.nt];
         for (size_t i = 0; i < c.nt; ++i) P->rows[t0 + i + 1] = cc.r0 + r[i + 1];
         RT_TRY(rt_search_plan_prepare(cc.plan));
+        RT_TRY(rt_search_set_graph(cc.plan, 1));  // each chunk always uses the same buffers
     }
     size_t max_s = 1, max_r = 1;
     for (const Chunk& c : P->chunks) {
