@@ -364,16 +364,16 @@ __device__ __forceinline__ void level_rows_unrolled(const RowOp* ops, int nrows,
             }
         } else {
             const float* Tr = src + (size_t)op.t * sstride;
+            // idx = (shift + 32 j + lane) mod b, stepped by 32 (one wrap at most: b > 32)
+            int idx = op.shift + lane;
+            idx -= (idx >= b) ? b : 0;
 #pragma unroll
             for (int j = 0; j < NIT; ++j) {
                 const int c = lane + 32 * j;
-                if (j < NIT - 1 || c < b) {
-                    int p0 = 32 * j + op.shift;
-                    p0 -= (p0 >= b) ? b : 0;
-                    int idx = p0 + lane;
-                    idx -= (idx >= b) ? b : 0;
+                if (j < NIT - 1 || c < b)
                     v[j] = __fadd_rn(kGlobal ? __ldcg(H + c) : H[c], kGlobal ? __ldcg(Tr + idx) : Tr[idx]);
-                }
+                idx += 32;
+                idx -= (idx >= b) ? b : 0;
             }
         }
 #pragma unroll
@@ -398,18 +398,18 @@ __device__ __forceinline__ void level_rows_pairs(const RowOp* ops, int nrows,
         float* out = dst + (size_t)r * stride;
         const float* H = src + (size_t)op.h * sstride + lane;
         const float* Tr = src + (size_t)op.t * sstride;
+        // i0 = (shift + 64 j + lane) mod b, stepped by 64 per chunk (one wrap at most: b > 64)
+        int i0 = op.shift + lane;
+        i0 -= (i0 >= b) ? b : 0;
 #pragma unroll
         for (int j = 0; j < NIT2; ++j) {
-            int p0 = op.shift + 64 * j;  // < b + 64 j: at most two wraps for NIT2 <= 9
-            p0 -= (p0 >= b) ? b : 0;
-            p0 -= (p0 >= b) ? b : 0;
             const int c = 64 * j + lane;
-            int i0 = p0 + lane;
-            i0 -= (i0 >= b) ? b : 0;
             int i1 = i0 + 32;
             i1 -= (i1 >= b) ? b : 0;
             if (j < NIT2 - 1 || c < b) out[c] = __fadd_rn(H[64 * j], Tr[i0]);
             if (j < NIT2 - 1 || c + 32 < b) out[c + 32] = __fadd_rn(H[64 * j + 32], Tr[i1]);
+            i0 += 64;
+            i0 -= (i0 >= b) ? b : 0;
         }
     }
 }
