@@ -51,12 +51,15 @@ struct JobTree {
     int depth;                          // G: nodes at this level read the global source
     int error;                          // nonzero if the job does not fit
     // Source rows of level G staged in shared memory (jobs of later stages, whose source is
-    // the previous stage's output with 16-byte aligned rows): node i of level G reads its
-    // head child's rows [hlo, hhi) from staged rows src_off[i] + (h - hlo) and its tail
-    // child's rows [tlo, thi) right after them. pstaged = 0: level G reads global rows.
+    // the previous stage's output with 16-byte aligned rows; G <= kMaxStagedDepth): node i
+    // of level G reads its head child's source rows src_rng[i].x + [0, src_rng[i].y) from
+    // staged rows src_off[i] + ..., and its tail child's rows src_rng[i].z + [0, .w) right
+    // after them. pstaged = 0: level G reads global rows.
     int pstaged;
-    int src_off[(kMaxJobNodes + 1) / 2 + 1];
+    int src_off[33];
+    int4 src_rng[32];
 };
+constexpr int kMaxStagedDepth = 5;
 
 // Description of one job, produced by the planners (host).
 struct JobSpec {
@@ -235,37 +238,41 @@ __device__ inline void build_job_tree_warp(JobTree& T, const JobSpec& J, int cap
         acc += carry;
     }
     if (lane == 0) T.op_start[G + 1] = acc;
-    if (stage_source) {
+    if (stage_source && G <= kMaxStagedDepth) {
         // rows each level-G node needs from its two children, as consecutive staged blocks
+        // (one lane per node: at most 32 nodes)
         const int n = 1 << G, base = n - 1;
-        int carry = 0;
+        const int i = lane;
+        int v = 0;
         bool two = true;
-        for (int b0 = 0; b0 < n; b0 += 32) {
-            const int i = b0 + lane;
-            int v = 0;
-            if (i < n) {
-                const Node nd = T.nodes[base + i];
-                if (nd.rows < 2) {
-                    two = false;
-                } else if (nd.hi > nd.lo) {
-                    const MergeCoef c = merge_coef(nd.rows);
-                    v = (merge_row(c.kh, nd.hi - 1) + 1 - merge_row(c.kh, nd.lo)) +
-                        (merge_row(c.kt, nd.hi - 1) + 1 - merge_row(c.kt, nd.lo));
-                }
+        if (i < n) {
+            const Node nd = T.nodes[base + i];
+            int4 rg = make_int4(nd.row0, 0, nd.row0 + (nd.rows >> 1), 0);
+            if (nd.rows < 2) {
+                two = false;
+            } else if (nd.hi > nd.lo) {
+                const MergeCoef c = merge_coef(nd.rows);
+                const int hlo = merge_row(c.kh, nd.lo), tlo = merge_row(c.kt, nd.lo);
+                rg.x += hlo;
+                rg.y = merge_row(c.kh, nd.hi - 1) + 1 - hlo;
+                rg.z += tlo;
+                rg.w = merge_row(c.kt, nd.hi - 1) + 1 - tlo;
             }
-            int incl = v;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += y;
-            }
-            if (i < n) T.src_off[i] = carry + incl - v;
-            carry += __shfl_sync(0xffffffffu, incl, 31);
+            v = rg.y + rg.w;
+            T.src_rng[i] = rg;
         }
+        int incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (i < n) T.src_off[i] = incl - v;
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
         two = __all_sync(0xffffffffu, two);
         if (lane == 0) {
-            T.src_off[n] = carry;
-            T.pstaged = (two && carry <= cap_rows) ? 1 : 0;
+            T.src_off[n] = total;
+            T.pstaged = (two && total <= cap_rows) ? 1 : 0;
         }
     }
     __syncwarp();
@@ -314,10 +321,9 @@ __device__ __forceinline__ RowOp make_row_op(const JobTree& T, int d, int r, int
         const int h = merge_row(c.kh, s), t = merge_row(c.kt, s);
         op.shift = (s - t) % b;
         if (d == T.depth && T.pstaged) {
-            const int hlo = merge_row(c.kh, nd.lo);
-            const int hn = merge_row(c.kh, nd.hi - 1) + 1 - hlo;
-            op.h = T.src_off[i] + (h - hlo);
-            op.t = T.src_off[i] + hn + (t - merge_row(c.kt, nd.lo));
+            const int4 rg = T.src_rng[i];
+            op.h = T.src_off[i] + (nd.row0 + h - rg.x);
+            op.t = T.src_off[i] + rg.y + (nd.row0 + (nd.rows >> 1) + t - rg.z);
         } else if (d == T.depth) {
             op.h = nd.row0 + h;
             op.t = nd.row0 + (nd.rows >> 1) + t;
@@ -542,7 +548,7 @@ __device__ inline void stage_source_rows_async(const JobTree& T, const float* sr
                                                float* sbuf, uint64_t* bar)
 {
     const int lane = threadIdx.x & 31;
-    const int G = T.depth, n = 1 << G, base = n - 1;
+    const int n = 1 << T.depth;
     const size_t row_bytes = (size_t)stride * sizeof(float);
     // the source was written by other CTAs (generic proxy) before they signalled it
     asm volatile("fence.proxy.async.global;" ::: "memory");
@@ -551,13 +557,9 @@ __device__ inline void stage_source_rows_async(const JobTree& T, const float* sr
     __syncwarp();
     constexpr uint32_t kChunk = 32768;
     for (int i = lane; i < n; i += 32) {
-        const Node nd = T.nodes[base + i];
-        if (nd.hi <= nd.lo) continue;
-        const MergeCoef c = merge_coef(nd.rows);
-        const int hlo = merge_row(c.kh, nd.lo), hn = merge_row(c.kh, nd.hi - 1) + 1 - hlo;
-        const int tlo = merge_row(c.kt, nd.lo), tn = merge_row(c.kt, nd.hi - 1) + 1 - tlo;
-        const int r0[2] = {nd.row0 + hlo, nd.row0 + (nd.rows >> 1) + tlo};
-        const int cnt[2] = {hn, tn};
+        const int4 rg = T.src_rng[i];
+        const int r0[2] = {rg.x, rg.z};
+        const int cnt[2] = {rg.y, rg.w};
         int off = T.src_off[i];
         for (int h = 0; h < 2; ++h) {
             const unsigned char* from =
