@@ -157,6 +157,17 @@ int rt_search_plan_create(const uint64_t* h_lengths, size_t ntrials,
 /* Row offsets of each trial in the packed outputs: ntrials + 1 entries. */
 int rt_search_plan_rows(const rt_search_plan* plan, uint64_t* h_row_offsets);
 int rt_search_plan_stats(const rt_search_plan* plan, rt_search_plan_stats_t* stats);
+/* Description of one (trial, octave cycle, bins) transform of a plan: its periodogram rows
+ * are out_row + [0, rows_eval) of the packed outputs; the series is downsampled by `factor`
+ * (1: not downsampled) and folded into rows x bins. num_transforms entries (plan stats). */
+typedef struct rt_search_transform {
+    uint32_t trial, cycle, bins, rows, rows_eval;
+    uint64_t out_row;
+    double factor;
+    double tau;
+    float stdnoise;
+} rt_search_transform;
+int rt_search_plan_transforms(const rt_search_plan* plan, rt_search_transform* h_out);
 /* Allocates and uploads the plan's device buffers now (otherwise the first run does it;
  * cudaMalloc synchronises the device, so do this before timing or overlapping work). */
 int rt_search_plan_prepare(rt_search_plan* plan);
@@ -218,6 +229,31 @@ int rt_search_pipeline_run(rt_search_pipeline* pipeline, const float* h_data,
 /* Synchronises `stream` and reports a device-side failure of any chunk. */
 int rt_search_pipeline_check(rt_search_pipeline* pipeline, void* stream);
 void rt_search_pipeline_destroy(rt_search_pipeline* pipeline);
+
+/* ---------------------------------------------------------------------------------
+ * Adjoints of the search steps, for gradients of a loss of the periodogram with respect to
+ * the searched series (differentiable search; no counterpart in the reference, whose search
+ * is not differentiable). Each computes the transpose of the Jacobian of the forward step
+ * named, applied to an output gradient.
+ * -------------------------------------------------------------------------------*/
+/* snr2 (snr.hpp:37-65): gradient with respect to the rows x cols profiles d_in, given the
+ * gradient d_gsnr (rows x num_widths) of the S/N. The max over phases is routed to its first
+ * maximising phase (per row and width); sum and dmax as the forward computes them. */
+int rt_snr2_backward(const float* d_in, size_t rows, size_t cols, const uint64_t* h_widths,
+                     size_t num_widths, float stdnoise, const float* d_gsnr, float* d_gin,
+                     void* stream);
+/* ffa2 (transforms.hpp:13-61): d_gin = FFA^T d_gout for a rows x cols block (the transposed
+ * butterfly: each level's gradient gathered from the rows that read it, rolls reversed). */
+int rt_ffa2_transpose(const float* d_gout, size_t rows, size_t cols, float* d_gin, void* stream);
+/* downsample (downsample.hpp:44-82): d_gin[i] += sum_k w(k, i) d_gout[k] over the
+ * floor(size / f) outputs, the same FP64 bounds and float32 edge weights as the forward.
+ * Accumulates into d_gin (size values). */
+int rt_downsample_adjoint(const float* d_gout, size_t size, double f, float* d_gin,
+                          void* stream);
+/* normalise (time_series.py:67-93), z = (y - mean) / std with population std:
+ * d_gy = (g - mean(g) - z * mean(g z)) / std, with d_z the normalised series. */
+int rt_normalise_adjoint(const float* d_g, const float* d_z, size_t size, double std_,
+                         float* d_gy, void* stream);
 
 #ifdef __cplusplus
 }

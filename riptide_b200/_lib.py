@@ -51,6 +51,11 @@ SIGNATURES = {
     "rt_search_phase_cycles": (ctypes.c_int, [_vp, _u64p, ctypes.c_int]),
     "rt_search_plan_destroy": (None, [_vp]),
     "rt_search_plan_prepare": (ctypes.c_int, [_vp]),
+    "rt_search_plan_transforms": (ctypes.c_int, [_vp, _vp]),
+    "rt_snr2_backward": (ctypes.c_int, [_vp, _sz, _sz, _u64p, _sz, ctypes.c_float, _vp, _vp, _vp]),
+    "rt_ffa2_transpose": (ctypes.c_int, [_vp, _sz, _sz, _vp, _vp]),
+    "rt_downsample_adjoint": (ctypes.c_int, [_vp, _sz, _d, _vp, _vp]),
+    "rt_normalise_adjoint": (ctypes.c_int, [_vp, _vp, _sz, _d, _vp, _vp]),
     "rt_search_set_graph": (ctypes.c_int, [_vp, ctypes.c_int]),
     "rt_search_graph_captures": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
     "rt_search_pipeline_create": (ctypes.c_int, [_u64p, _sz, _vp, _u64p, _sz, _sz, ctypes.POINTER(_vp)]),
@@ -81,6 +86,13 @@ class PlanStats(ctypes.Structure):
         "num_trials", "num_cycles", "num_transforms", "num_work_items", "num_multistage",
         "total_rows", "total_samples", "downsampled_samples", "folded_samples",
         "scrunch_factor")]
+
+
+class SearchTransform(ctypes.Structure):
+    _fields_ = [("trial", ctypes.c_uint32), ("cycle", ctypes.c_uint32), ("bins", ctypes.c_uint32),
+                ("rows", ctypes.c_uint32), ("rows_eval", ctypes.c_uint32),
+                ("out_row", ctypes.c_uint64), ("factor", ctypes.c_double), ("tau", ctypes.c_double),
+                ("stdnoise", ctypes.c_float)]
 
 
 class RiptideError(RuntimeError):

@@ -747,6 +747,7 @@ struct SearchPlan {
     // work
     std::vector<StagePlan> plans;
     std::vector<XformRec> xforms;
+    std::vector<int2> xform_tc;          // (trial, cycle) of each transform
     std::vector<WorkItem> items;
     int nseq = 0;
     size_t slot_floats = 0;
@@ -926,6 +927,7 @@ static int plan_build(SearchPlan& P)
                     if (X.seq >= kSlots) finish_seq(X.seq - kSlots);
                 }
                 P.xforms.push_back(X);
+                P.xform_tc.push_back(make_int2(t, ci));
                 rows_total += re;
                 emit_stage(xi, 0);
                 flush();
@@ -1315,6 +1317,26 @@ extern "C" int rt_search_graph_captures(const rt_search_plan* plan, int* h_count
 {
     if (!plan || !h_count) return set_error(RT_EINVAL, "null argument");
     *h_count = plan->p.graph_captures;
+    return RT_OK;
+}
+
+extern "C" int rt_search_plan_transforms(const rt_search_plan* plan, rt_search_transform* h_out)
+{
+    if (!plan || !h_out) return set_error(RT_EINVAL, "null argument");
+    const SearchPlan& P = plan->p;
+    for (size_t i = 0; i < P.xforms.size(); ++i) {
+        const XformRec& X = P.xforms[i];
+        rt_search_transform& o = h_out[i];
+        o.trial = (uint32_t)P.xform_tc[i].x;
+        o.cycle = (uint32_t)P.xform_tc[i].y;
+        o.bins = (uint32_t)X.b;
+        o.rows = (uint32_t)X.m;
+        o.rows_eval = (uint32_t)X.rows_eval;
+        o.out_row = X.out_row;
+        o.factor = P.f[P.xform_tc[i].y];
+        o.tau = X.tau;
+        o.stdnoise = X.stdnoise;
+    }
     return RT_OK;
 }
 
