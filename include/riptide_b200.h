@@ -168,6 +168,9 @@ typedef struct rt_search_transform {
     float stdnoise;
 } rt_search_transform;
 int rt_search_plan_transforms(const rt_search_plan* plan, rt_search_transform* h_out);
+/* Per-trial mean and (population) standard deviation of the series the last run normalised
+ * (after deredden); 0 and 1 when the plan does not normalise. Synchronises `stream`. */
+int rt_search_normalisation(rt_search_plan* plan, double* h_mean, double* h_std, void* stream);
 /* Allocates and uploads the plan's device buffers now (otherwise the first run does it;
  * cudaMalloc synchronises the device, so do this before timing or overlapping work). */
 int rt_search_plan_prepare(rt_search_plan* plan);
@@ -250,6 +253,16 @@ int rt_ffa2_transpose(const float* d_gout, size_t rows, size_t cols, float* d_gi
  * Accumulates into d_gin (size values). */
 int rt_downsample_adjoint(const float* d_gout, size_t size, double f, float* d_gin,
                           void* stream);
+/* Gradient with respect to the searched series of sum(d_gsnr * snrs) for the last run of
+ * `plan`, when few periodogram rows carry a gradient (a max-S/N loss: one row per trial):
+ * each such row is recomputed from the downsampled series the run left in the plan (so the
+ * plan must not have run again since), its boxcar S/N differentiated, and the row gradient
+ * taken back through the FFA's shifts and the downsampling. d_z: the normalised series the
+ * run searched (rt_search_run's d_normalised); d_gsnr: L x num_widths; d_gz (output, packed
+ * like the input) is the gradient with respect to d_z. RT_EINVAL when more than max_rows
+ * rows carry a gradient (use the per-transform adjoints instead). */
+int rt_search_backward_rows(rt_search_plan* plan, const float* d_z, const float* d_gsnr,
+                            float* d_gz, size_t max_rows, void* stream);
 /* normalise (time_series.py:67-93), z = (y - mean) / std with population std:
  * d_gy = (g - mean(g) - z * mean(g z)) / std, with d_z the normalised series. */
 int rt_normalise_adjoint(const float* d_g, const float* d_z, size_t size, double std_,

@@ -1171,6 +1171,334 @@ static int plan_check_error(SearchPlan& P, cudaStream_t st)
     return RT_OK;
 }
 
+// ------------------------------------------------------------------------------------
+// Sparse-row backward of a run: the gradient with respect to the searched (normalised)
+// series of sum(gsnr * snrs), for gradients on few periodogram rows (a max-S/N loss has one
+// per trial). Output row s of a transform is a sum of every input row i rolled by a total
+// shift sigma_i(s) (the tail shifts met on the way from the root to leaf i); the row is
+// recomputed from the downsampled series that the run left in its arena, its boxcar S/N is
+// differentiated (the max routed to the first maximising phase), and the row gradient is
+// scattered back through the same shifts, then through the downsampling.
+// ------------------------------------------------------------------------------------
+struct BwdJob {
+    int m, b, s, pad;
+    float stdnoise;
+    int pad2;
+    unsigned long long grow;  // row index into gsnr
+};
+
+struct BwdGroup {
+    unsigned long long src;   // float offset of the folded series (arena or z)
+    unsigned long long gds;   // float offset of this group's downsampled gradient
+    unsigned long long gz;    // float offset of the trial's series in the packed gradient
+    unsigned long long sig;   // int offset of this group's shift table
+    int job0, njobs, src_is_z, pad;
+    size_t n_ds, N;
+    double f;
+};
+
+constexpr int kBwdThreads = 256;
+constexpr int kBwdMaxBins = 4096;
+
+__global__ void __launch_bounds__(kBwdThreads)
+    k_rows_backward(const BwdGroup* __restrict__ groups, const BwdJob* __restrict__ jobs,
+                    const float* __restrict__ arena, const float* __restrict__ z,
+                    const float* __restrict__ gsnr, const int* __restrict__ widths, int nw,
+                    int wmax, float* __restrict__ gds_all, int* __restrict__ sig_all)
+{
+    extern __shared__ float sm[];
+    float* F = sm;                       // kBwdMaxBins
+    float* C = F + kBwdMaxBins;          // b + wmax
+    __shared__ float s_g[kBwdMaxBins];
+    __shared__ int s_best[64];
+    const BwdGroup G = groups[blockIdx.x];
+    const float* src = (G.src_is_z ? z : arena) + G.src;
+    float* gds = gds_all + G.gds;
+    int* sig = sig_all + G.sig;
+    const int tid = threadIdx.x, lane = tid & 31;
+    for (int q = 0; q < G.njobs; ++q) {
+        const BwdJob J = jobs[G.job0 + q];
+        const int m = J.m, b = J.b;
+        // total shift of every input row for output row s
+        for (int i = tid; i < m; i += kBwdThreads) {
+            int row0 = 0, n = m, r = J.s, sg = 0;
+            while (n > 1) {
+                const int nh = n >> 1;
+                const MergeCoef mc = merge_coef(n);
+                const int h = merge_row(mc.kh, r), t = merge_row(mc.kt, r);
+                if (i < row0 + nh) {
+                    n = nh;
+                    r = h;
+                } else {
+                    sg += (r - t) % b;
+                    sg -= (sg >= b) ? b : 0;
+                    row0 += nh;
+                    n -= nh;
+                    r = t;
+                }
+            }
+            sig[i] = sg;
+        }
+        __syncthreads();
+        // the output row
+        for (int c = tid; c < b; c += kBwdThreads) {
+            float acc = 0.0f;
+            for (int i = 0; i < m; ++i) {
+                int idx = c + sig[i];
+                idx -= (idx >= b) ? b : 0;
+                acc = __fadd_rn(acc, src[(size_t)i * b + idx]);
+            }
+            F[c] = acc;
+        }
+        __syncthreads();
+        // boxcar S/N backward of the row (one warp)
+        if (tid < 32) {
+            double carry = 0.0;
+            for (int c0 = 0; c0 < b; c0 += 32) {
+                const int c = c0 + lane;
+                const double v = (c < b) ? (double)F[c] : 0.0;
+                double incl = v;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const double y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                if (c < b) C[c] = (float)(carry + incl);
+                carry += __shfl_sync(0xffffffffu, incl, 31);
+            }
+            __syncwarp();
+            const float sumx = (float)carry;
+            for (int j = lane; j < wmax; j += 32) C[b + j] = __fadd_rn(C[j], sumx);
+            __syncwarp();
+            for (int k = 0; k < nw; ++k) {
+                const int w = widths[k];
+                float best = -INFINITY;
+                int bi = b;
+                for (int i = lane; i < b; i += 32) {
+                    const float d = __fsub_rn(C[i + w], C[i]);
+                    if (d > best) {
+                        best = d;
+                        bi = i;
+                    }
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const float ob = __shfl_xor_sync(0xffffffffu, best, o);
+                    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                    if (ob > best || (ob == best && oi < bi)) {
+                        best = ob;
+                        bi = oi;
+                    }
+                }
+                if (lane == 0) s_best[k] = bi;
+            }
+        }
+        __syncthreads();
+        const float* g = gsnr + (size_t)J.grow * nw;
+        for (int c = tid; c < b; c += kBwdThreads) {
+            double acc = 0.0;
+            for (int k = 0; k < nw; ++k) {
+                float hb, be;
+                boxcar_coefs(b, widths[k], &hb, &be);
+                acc -= (double)g[k] * (double)be;
+                int off = c - s_best[k] - 1;
+                off += (off < 0) ? b : 0;
+                if (off < widths[k]) acc += (double)g[k] * (double)hb;
+            }
+            s_g[c] = (float)(acc / (double)J.stdnoise);
+        }
+        __syncthreads();
+        // back through the shifts: row i reads the row gradient at c - sigma_i
+        for (size_t e = tid; e < (size_t)m * b; e += kBwdThreads) {
+            const int i = (int)(e / b), c = (int)(e - (size_t)i * b);
+            int idx = c - sig[i];
+            idx += (idx < 0) ? b : 0;
+            gds[e] = __fadd_rn(gds[e], s_g[idx]);
+        }
+        __syncthreads();
+    }
+}
+
+// Downsampling adjoint of the groups of one wave (each trial at most once per wave).
+__global__ void k_groups_ds_adjoint(const BwdGroup* __restrict__ groups, const int* __restrict__ wave,
+                                    const float* __restrict__ gds_all, float* __restrict__ gz_all)
+{
+    const BwdGroup G = groups[wave[blockIdx.y]];
+    const float* gout = gds_all + G.gds;
+    float* gin = gz_all + G.gz;
+    const size_t N = G.N, n = G.n_ds;
+    const double f = G.f;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N;
+         i += (size_t)gridDim.x * blockDim.x) {
+        if (G.src_is_z) {  // the cycle folds the series itself
+            if (i < n) gin[i] = __fadd_rn(gin[i], gout[i]);
+            continue;
+        }
+        const double qf = floor((double)i / f);
+        const size_t k0 = qf >= 1.0 ? (size_t)qf - 1 : 0;
+        const size_t k1 = min(n, (size_t)floor((double)(i + 1) / f) + 2);
+        double acc = 0.0;
+        for (size_t k = k0; k < k1; ++k) {
+            const double start = (double)k * f;
+            const double end = start + f;
+            const size_t imin = (size_t)floor(start);
+            const double fe = floor(end);
+            const size_t imax = (size_t)(fe < (double)N - 1.0 ? fe : (double)N - 1.0);
+            double c = 0.0;
+            if (i == imin) c += (double)__double2float_rn((double)(imin + 1) - start);
+            if (i == imax) c += (double)__double2float_rn(end - (double)imax);
+            if (i > imin && i < imax) c += 1.0;
+            if (imax == imin && i == imin) c -= 1.0;
+            if (c != 0.0) acc += c * (double)gout[k];
+        }
+        if (acc != 0.0) gin[i] = __fadd_rn(gin[i], (float)acc);
+    }
+}
+
+__global__ void k_live_rows(const float* __restrict__ g, size_t rows, int nw,
+                            unsigned long long* __restrict__ list, unsigned long long cap,
+                            unsigned long long* __restrict__ count)
+{
+    for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < rows;
+         r += (size_t)gridDim.x * blockDim.x) {
+        bool live = false;
+        for (int k = 0; k < nw; ++k) live |= g[r * nw + k] != 0.0f;
+        if (live) {
+            const unsigned long long slot = atomicAdd(count, 1ull);
+            if (slot < cap) list[slot] = r;
+        }
+    }
+}
+
+static int plan_backward(SearchPlan& P, const float* d_z, const float* d_gsnr, float* d_gz,
+                         size_t max_rows, cudaStream_t st)
+{
+    if (!P.dev_ready) return set_error(RT_EINVAL, "the plan has not run");
+    const size_t L = P.out_rows_off.back();
+    const int nw = (int)P.widths.size();
+    RT_TRY_CUDA(cudaMemsetAsync(d_gz, 0, P.total_len * sizeof(float), st));
+    if (L == 0 || nw == 0) return RT_OK;
+    // rows that carry a gradient
+    unsigned long long *d_list = nullptr, *d_count = nullptr;
+    RT_TRY_CUDA(cudaMallocAsync((void**)&d_list, (max_rows + 1) * sizeof(unsigned long long), st));
+    d_count = d_list + max_rows;
+    RT_TRY_CUDA(cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), st));
+    k_live_rows<<<(unsigned)std::min<size_t>((L + 255) / 256, 148 * 16), 256, 0, st>>>(
+        d_gsnr, L, nw, d_list, max_rows, d_count);
+    unsigned long long count = 0;
+    RT_TRY_CUDA(cudaMemcpyAsync(&count, d_count, sizeof(count), cudaMemcpyDeviceToHost, st));
+    RT_TRY_CUDA(cudaStreamSynchronize(st));
+    if (count > max_rows) {
+        cudaFreeAsync(d_list, st);
+        return set_error(RT_EINVAL, "%llu periodogram rows carry a gradient (at most %zu)", count,
+                         max_rows);
+    }
+    std::vector<unsigned long long> rows(count);
+    if (count)
+        RT_TRY_CUDA(cudaMemcpyAsync(rows.data(), d_list, count * sizeof(unsigned long long),
+                                    cudaMemcpyDeviceToHost, st));
+    RT_TRY_CUDA(cudaStreamSynchronize(st));
+    cudaFreeAsync(d_list, st);
+    if (count == 0) return RT_OK;
+    std::sort(rows.begin(), rows.end());
+    // rows -> (transform, s), grouped by (trial, cycle) in plan order
+    const int C = (int)P.f.size();
+    std::vector<BwdJob> jobs;
+    std::vector<BwdGroup> groups;
+    std::vector<int> group_trial;
+    size_t xi = 0, gds_total = 0, sig_total = 0;
+    int last_tc = -1;
+    for (unsigned long long r : rows) {
+        while (xi + 1 < P.xforms.size() && P.xforms[xi + 1].out_row <= r) ++xi;
+        const XformRec& X = P.xforms[xi];
+        if (r < X.out_row || r >= X.out_row + (unsigned long long)X.rows_eval) continue;
+        if (X.b > kBwdMaxBins || X.b + (size_t)*std::max_element(P.widths.begin(), P.widths.end()) > 2 * kBwdMaxBins)
+            return set_error(RT_EINVAL, "profiles of %d bins are too long for the backward", X.b);
+        const int t = P.xform_tc[xi].x, c = P.xform_tc[xi].y;
+        const int tc = t * C + c;
+        if (tc != last_tc) {
+            BwdGroup G;
+            const double f = P.f[c];
+            const size_t N = P.lengths[t];
+            G.src_is_z = (f == 1) ? 1 : 0;
+            G.src = G.src_is_z ? P.offsets[t] : P.ds_off[(size_t)tc];
+            G.n_ds = G.src_is_z ? N : downsampled_size(N, f);
+            G.N = N;
+            G.f = f;
+            G.gds = gds_total;
+            gds_total += (G.n_ds + 3) & ~size_t(3);
+            G.gz = P.offsets[t];
+            G.sig = sig_total;
+            G.job0 = (int)jobs.size();
+            G.njobs = 0;
+            G.pad = 0;
+            groups.push_back(G);
+            group_trial.push_back(t);
+            last_tc = tc;
+        }
+        BwdGroup& G = groups.back();
+        BwdJob J;
+        J.m = X.m;
+        J.b = X.b;
+        J.s = (int)(r - X.out_row);
+        J.stdnoise = X.stdnoise;
+        J.grow = r;
+        J.pad = J.pad2 = 0;
+        jobs.push_back(J);
+        ++G.njobs;
+        sig_total = std::max<size_t>(sig_total, (size_t)G.sig + (size_t)X.m);
+    }
+    if (jobs.empty()) return RT_OK;
+    // waves: the k-th group of every trial (a trial's groups accumulate into one series)
+    std::vector<std::vector<int>> waves;
+    {
+        std::map<int, int> seen;
+        for (size_t g = 0; g < groups.size(); ++g) {
+            const int k = seen[group_trial[g]]++;
+            if ((int)waves.size() <= k) waves.emplace_back();
+            waves[k].push_back((int)g);
+        }
+    }
+    int wmax = 1;
+    for (int w : P.widths) wmax = std::max(wmax, w);
+    unsigned char* blob = nullptr;
+    const size_t nwave = groups.size();
+    const size_t bytes = groups.size() * sizeof(BwdGroup) + jobs.size() * sizeof(BwdJob) +
+                         nwave * sizeof(int) + (gds_total + 4) * sizeof(float) +
+                         (sig_total + 4) * sizeof(int) + 64;
+    RT_TRY_CUDA(cudaMallocAsync((void**)&blob, bytes, st));
+    BwdGroup* d_groups = reinterpret_cast<BwdGroup*>(blob);
+    BwdJob* d_jobs = reinterpret_cast<BwdJob*>(d_groups + groups.size());
+    int* d_wave = reinterpret_cast<int*>(d_jobs + jobs.size());
+    float* d_gds = reinterpret_cast<float*>(
+        (reinterpret_cast<uintptr_t>(d_wave + nwave) + 15) & ~uintptr_t(15));
+    int* d_sig = reinterpret_cast<int*>(d_gds + gds_total + 4);
+    int s = RT_OK;
+    auto ck = [&](cudaError_t e) { if (s == RT_OK && e != cudaSuccess) s = check_cuda(e, "search backward"); };
+    ck(cudaMemcpyAsync(d_groups, groups.data(), groups.size() * sizeof(BwdGroup),
+                       cudaMemcpyHostToDevice, st));
+    ck(cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(BwdJob), cudaMemcpyHostToDevice, st));
+    ck(cudaMemsetAsync(d_gds, 0, gds_total * sizeof(float), st));
+    const size_t smem = (size_t)(2 * kBwdMaxBins + wmax) * sizeof(float);
+    ck(cudaFuncSetAttribute(k_rows_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (s == RT_OK) {
+        k_rows_backward<<<(unsigned)groups.size(), kBwdThreads, smem, st>>>(
+            d_groups, d_jobs, P.d_ds, d_z, d_gsnr, P.d_widths, nw, wmax, d_gds, d_sig);
+        ck(cudaGetLastError());
+    }
+    // every group of a kernel call uses its own shift table: the groups run concurrently
+    (void)sig_total;
+    for (const auto& w : waves) {
+        if (s != RT_OK) break;
+        ck(cudaMemcpyAsync(d_wave, w.data(), w.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        dim3 grid(64, (unsigned)w.size());
+        k_groups_ds_adjoint<<<grid, 256, 0, st>>>(d_groups, d_wave, d_gds, d_gz);
+        ck(cudaGetLastError());
+    }
+    cudaFreeAsync(blob, st);
+    return s;
+}
+
 }  // namespace rt
 
 // ====================================================================================
@@ -1338,6 +1666,35 @@ extern "C" int rt_search_plan_transforms(const rt_search_plan* plan, rt_search_t
         o.stdnoise = X.stdnoise;
     }
     return RT_OK;
+}
+
+extern "C" int rt_search_normalisation(rt_search_plan* plan, double* h_mean, double* h_std,
+                                       void* stream)
+{
+    if (!plan || !h_mean || !h_std) return set_error(RT_EINVAL, "null argument");
+    SearchPlan& P = plan->p;
+    const size_t T = P.lengths.size();
+    if (!P.dev_ready || P.cfg.already_normalised) {
+        for (size_t t = 0; t < T; ++t) {
+            h_mean[t] = 0.0;
+            h_std[t] = 1.0;
+        }
+        return RT_OK;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    RT_TRY_CUDA(cudaMemcpyAsync(h_mean, P.d_mean, T * sizeof(double), cudaMemcpyDeviceToHost, st));
+    RT_TRY_CUDA(cudaMemcpyAsync(h_std, P.d_normv, T * sizeof(double), cudaMemcpyDeviceToHost, st));
+    RT_TRY_CUDA(cudaStreamSynchronize(st));
+    return RT_OK;
+}
+
+extern "C" int rt_search_backward_rows(rt_search_plan* plan, const float* d_z,
+                                       const float* d_gsnr, float* d_gz, size_t max_rows,
+                                       void* stream)
+{
+    if (!plan || !d_z || !d_gsnr || !d_gz) return set_error(RT_EINVAL, "null argument");
+    if (max_rows == 0) return set_error(RT_EINVAL, "max_rows must be positive");
+    return plan_backward(plan->p, d_z, d_gsnr, d_gz, max_rows, (cudaStream_t)stream);
 }
 
 extern "C" int rt_search_plan_prepare(rt_search_plan* plan)

@@ -84,21 +84,27 @@ def normalise_adjoint(g, z, std):
 
 
 def _rmed_adjoint(x, g, width_samples, min_points):
-    """(fast_running_median)^T g for a series x (running_medians.py:49-85): the gradient that
-    the subtracted running median takes away, through np.interp, the exact median of each
-    window (to the element it selects, edge-padded windows) and the scrunch mean."""
+    """(fast_running_median)^T g for series x, one per row of a 2D x (running_medians.py:
+    49-85): the gradient that the subtracted running median takes away, through np.interp,
+    the exact median of each window (to the element it selects, edge-padded windows) and the
+    scrunch mean."""
     torch = libcpp._t()
-    N = x.numel()
+    one = x.dim() == 1
+    if one:
+        x, g = x.view(1, -1), g.view(1, -1)
+    T, N = x.shape
+    dev = x.device
     k = int(max(1, width_samples / float(min_points)))
     w = width_samples if k == 1 else min_points
     if k == 1:
         lores = x.double()
         glo = g.double()
+        nl = N
     else:
         nl = N // k
-        lores = x[:nl * k].view(nl, k).double().mean(1)
+        lores = x[:, :nl * k].reshape(T, nl, k).double().mean(2)
         # np.interp^T from x_lores = j k + (k - 1) / 2 back to every sample
-        i = torch.arange(N, device=x.device, dtype=torch.float64)
+        i = torch.arange(N, device=dev, dtype=torch.float64)
         pos = (i - 0.5 * (k - 1)) / k
         j = torch.floor(pos).clamp(0, nl - 1).long()
         a = (pos - j.double()).clamp(0.0, 1.0)
@@ -106,22 +112,26 @@ def _rmed_adjoint(x, g, width_samples, min_points):
         a = torch.where(pos >= nl - 1, torch.zeros_like(a), a)
         j = torch.where(pos >= nl - 1, torch.full_like(j, nl - 1), j)
         gd = g.double()
-        glo = torch.zeros(nl, dtype=torch.float64, device=x.device)
-        glo.index_add_(0, j, gd * (1.0 - a))
-        glo.index_add_(0, (j + 1).clamp(max=nl - 1), gd * a)
-    n = lores.numel()
+        rows = (torch.arange(T, device=dev) * nl).view(T, 1)
+        glo = torch.zeros(T * nl, dtype=torch.float64, device=dev)
+        glo.index_add_(0, (rows + j).view(-1), (gd * (1.0 - a)).view(-1))
+        glo.index_add_(0, (rows + (j + 1).clamp(max=nl - 1)).view(-1), (gd * a).view(-1))
+        glo = glo.view(T, nl)
     half = w // 2
-    padded = torch.cat([lores[:1].expand(half), lores, lores[-1:].expand(half)])
-    win = padded.unfold(0, w, 1)  # (n, w)
-    sel = torch.median(win, dim=1).indices + torch.arange(n, device=x.device) - half
-    sel = sel.clamp(0, n - 1)
-    gsel = torch.zeros(n, dtype=torch.float64, device=x.device)
-    gsel.index_add_(0, sel, glo)
+    padded = torch.cat([lores[:, :1].expand(T, half), lores, lores[:, -1:].expand(T, half)], 1)
+    win = padded.unfold(1, w, 1)  # (T, nl, w)
+    sel = torch.median(win, dim=2).indices + torch.arange(nl, device=dev) - half
+    sel = sel.clamp(0, nl - 1) + (torch.arange(T, device=dev) * nl).view(T, 1)
+    gsel = torch.zeros(T * nl, dtype=torch.float64, device=dev)
+    gsel.index_add_(0, sel.view(-1), glo.reshape(-1))
+    gsel = gsel.view(T, nl)
     if k == 1:
-        return gsel.float()
-    out = torch.zeros(N, dtype=torch.float64, device=x.device)
-    out[:n * k] = (gsel / k).repeat_interleave(k)
-    return out.float()
+        out = gsel.float()
+    else:
+        out = torch.zeros((T, N), dtype=torch.float64, device=dev)
+        out[:, :nl * k] = (gsel / k).repeat_interleave(k, dim=1)
+        out = out.float()
+    return out.view(-1) if one else out
 
 
 class DifferentiableSearch(object):
@@ -148,67 +158,114 @@ class DifferentiableSearch(object):
         self.rmed_width_samples = int(round(rmed_width / self.tsamp))
         self.rmed_minpts = int(rmed_minpts)
 
-    def forward(self, x):
-        """(periods, foldbins, snrs) of the packed CUDA float32 series x (no autograd)."""
+    def forward(self, x, keep=False):
+        """(periods, foldbins, snrs) of the packed CUDA float32 series x (no autograd). With
+        keep, also (z, std): the searched (dereddened, normalised) series and the per-trial
+        standard deviation it was normalised by, which the backward uses."""
         torch = libcpp._t()
         outs = self.bs.allocate_outputs(x.device)
-        return self.bs.run(x.detach().contiguous(), outs)
+        z = torch.empty_like(x) if keep else None
+        outs = self.bs.run(x.detach().contiguous(), outs, normalised=z)
+        self._runs = getattr(self, "_runs", 0) + 1
+        if not keep:
+            return outs
+        T = self.bs.num_trials
+        mean = (ctypes.c_double * T)()
+        std = (ctypes.c_double * T)()
+        _lib.check(_lib.load().rt_search_normalisation(self.bs._plan, mean, std, libcpp._stream()))
+        return outs, (z, np.array(std[:], dtype=np.float64), self._runs)
 
     def snrs(self, x):
         return _SearchFn.apply(x, self)
 
     # ------------------------------------------------------------------
-    def _searched(self, xt):
-        """(dereddened series, normalised series, std) of one trial, as the forward searches it."""
-        torch = libcpp._t()
-        y = xt
-        if self.deredden:
-            y = torch.empty_like(xt)
-            _lib.check(_lib.load().rt_deredden(libcpp._ptr(xt), xt.numel(), self.tsamp,
-                                               self.kw["rmed_width"], self.rmed_minpts,
-                                               libcpp._ptr(y), libcpp._stream()))
-        if not self.normalise:
-            return y, y, 1.0
-        yd = y.double()
-        m = yd.mean()
-        std = float(torch.sqrt(((yd - m) ** 2).mean()))
-        z = ((yd - m) / std).float()
-        return y, z, std
+    # the sparse-row backward runs when at most this many periodogram rows carry a gradient
+    max_sparse_rows = 1 << 16
 
-    def backward(self, x, gsnrs):
-        """Gradient with respect to x of sum(gsnrs * snrs(x))."""
+    def backward(self, x, gsnrs, saved):
+        """Gradient with respect to x of sum(gsnrs * snrs(x)); `saved` = (z, std, run) from
+        forward(keep=True)."""
         torch = libcpp._t()
-        gx = torch.zeros_like(x)
+        z_all, stds, run = saved
         gs = gsnrs.detach().float().contiguous()
+        gz_all = None
+        if run == self._runs:  # the plan still holds this run's downsampled series
+            gz_all = torch.empty_like(x)
+            rc = _lib.load().rt_search_backward_rows(self.bs._plan, libcpp._ptr(z_all),
+                                                     libcpp._ptr(gs), libcpp._ptr(gz_all),
+                                                     self.max_sparse_rows, libcpp._stream())
+            if rc == _lib.RT_EINVAL and b"carry a gradient" in _lib.load().rt_last_error():
+                gz_all = None
+            else:
+                _lib.check(rc)
+        if gz_all is None:
+            gz_all = self._gz_per_transform(x, gs, z_all)
+        return self._through_front(x, gz_all, z_all, stds)
+
+    def _gz_per_transform(self, x, gs, z_all):
+        """Gradient with respect to the searched series, one transform at a time (any number of
+        rows; the FFA outputs are recomputed from the normalised series)."""
+        torch = libcpp._t()
+        gz_all = torch.zeros_like(x)
         live = (gs != 0).any(dim=1).cpu().numpy() if gs.numel() else np.zeros(0, bool)
-        by_trial = {}
-        for (t, c, b, m, re, row0, f, sn) in self.transforms:
-            if re and live[row0:row0 + re].any():
-                by_trial.setdefault(t, {}).setdefault(c, []).append((b, m, re, row0, f, sn))
-        for t, cycles in by_trial.items():
+        tr = self._tr_arrays()
+        cs = np.concatenate([[0], np.cumsum(live)])
+        hit = np.nonzero((tr[:, 4] > 0) & (cs[tr[:, 5] + tr[:, 4]] > cs[tr[:, 5]]))[0]
+        groups = {}
+        for i in hit:
+            (t, c, b, m, re, row0, f, sn) = self.transforms[i]
+            groups.setdefault((t, c), []).append((b, m, re, row0, f, sn))
+        for (t, c), items in groups.items():
             a, e = int(self.offsets[t]), int(self.offsets[t + 1])
-            xt = x[a:e].detach().contiguous()
+            z = z_all[a:e]
             N = e - a
-            y, z, std = self._searched(xt)
-            gz = torch.zeros(N, dtype=torch.float32, device=x.device)
-            for c, items in cycles.items():
-                f = items[0][4]
-                ds = z if f == 1 else libcpp.downsample(z, f)
-                gds = torch.zeros_like(ds)
-                for (b, m, re, row0, _, sn) in items:
-                    F = _ffa2(ds[:m * b].view(m, b))
-                    gF = torch.zeros_like(F)
-                    gF[:re] = snr2_backward(F[:re], self.widths, sn, gs[row0:row0 + re])
-                    gds[:m * b] += ffa2_transpose(gF).view(-1)
-                if f == 1:
-                    gz += gds
-                else:
-                    downsample_adjoint(gds, N, f, gz)
-            gy = normalise_adjoint(gz, z, std) if self.normalise else gz
-            if self.deredden:
-                gy = gy - _rmed_adjoint(xt, gy, self.rmed_width_samples, self.rmed_minpts)
-            gx[a:e] = gy
+            f = items[0][4]
+            ds = z if f == 1 else libcpp.downsample(z, f)
+            gds = torch.zeros_like(ds)
+            for (b, m, re, row0, _, sn) in items:
+                F = _ffa2(ds[:m * b].view(m, b))
+                gF = torch.zeros_like(F)
+                gF[:re] = snr2_backward(F[:re], self.widths, sn, gs[row0:row0 + re])
+                gds[:m * b] += ffa2_transpose(gF).view(-1)
+            if f == 1:
+                gz_all[a:e] += gds
+            else:
+                downsample_adjoint(gds, N, f, gz_all[a:e])
+        return gz_all
+
+    def _tr_arrays(self):
+        if getattr(self, "_tr", None) is None:
+            self._tr = np.array([[t[0], t[1], t[2], t[3], t[4], t[5]] for t in self.transforms],
+                                dtype=np.int64).reshape(-1, 6)
+        return self._tr
+
+    def _through_front(self, x, gz_all, z_all, stds):
+        """From the gradient with respect to the searched series to the one with respect to x:
+        normalisation, then deredden."""
+        torch = libcpp._t()
+        gx = torch.empty_like(x) if self.normalise else gz_all
+        if self.normalise:
+            for t in range(self.bs.num_trials):
+                a, e = int(self.offsets[t]), int(self.offsets[t + 1])
+                gx[a:e] = normalise_adjoint(gz_all[a:e], z_all[a:e], float(stds[t]))
+        if self.deredden:
+            gx = gx - self._rmed_adjoint_batch(x.detach(), gx)
         return gx
+
+    def _rmed_adjoint_batch(self, x, g):
+        """_rmed_adjoint over every trial: one batched call when all trials have the same
+        length, one call per trial otherwise."""
+        torch = libcpp._t()
+        L = self.lengths
+        if L.size > 1 and np.all(L == L[0]):
+            n = int(L[0])
+            return _rmed_adjoint(x.view(-1, n), g.view(-1, n), self.rmed_width_samples,
+                                 self.rmed_minpts).view(-1)
+        out = torch.empty_like(g)
+        for t in range(L.size):
+            a, e = int(self.offsets[t]), int(self.offsets[t + 1])
+            out[a:e] = _rmed_adjoint(x[a:e], g[a:e], self.rmed_width_samples, self.rmed_minpts)
+        return out
 
     def close(self):
         self.bs.close()
@@ -226,15 +283,94 @@ class _SearchFn(object):
             class Fn(torch.autograd.Function):
                 @staticmethod
                 def forward(ctx, xin, s):
-                    _, _, snrs = s.forward(xin)
+                    (_, _, snrs), (z, std, run) = s.forward(xin, keep=True)
                     ctx.s = s
-                    ctx.save_for_backward(xin)
+                    ctx.std = std
+                    ctx.run = run
+                    ctx.save_for_backward(xin, z)
                     return snrs
 
                 @staticmethod
                 def backward(ctx, g):
-                    (xin,) = ctx.saved_tensors
-                    return ctx.s.backward(xin, g), None
+                    xin, z = ctx.saved_tensors
+                    return ctx.s.backward(xin, g, (z, ctx.std, ctx.run)), None
 
             cls._fn = Fn
         return cls._fn.apply(x, search)
+
+
+def _bench_config4(ntrials=64, steps=3, warmup=2, taps=257):
+    """One training step of the differentiable-search workload: a learnable `taps`-tap FIR
+    front end on `ntrials` series of 2^20 samples (100 us; half carry a pulsar), the search,
+    loss = mean max-S/N of the injected series - mean over the noise-only ones. Returns a
+    dict of CUDA-event times (ms) of the forward (FIR + search + loss) and the backward."""
+    import torch
+
+    from . import synth
+
+    cfg = synth.CONFIGS[4]
+    data, lengths, infos = synth.make_batch(4, ntrials)
+    n = int(lengths[0])
+    inj = torch.tensor([len(i["pulsars"]) > 0 for i in infos], device=data.device)
+    ds = DifferentiableSearch(lengths, cfg["tsamp"], **cfg["search"])
+    h = torch.zeros(taps, device=data.device)
+    h[taps // 2] = 1.0
+    h.requires_grad_(True)
+    rows = torch.from_numpy(ds.row_offsets).to(data.device)
+    trial_of_row = torch.repeat_interleave(torch.arange(ntrials, device=data.device),
+                                           rows[1:] - rows[:-1])
+
+    # FIR front end ('same' convolution) through FFTs: the weight gradient of a long 1-channel
+    # convolution is slow through the direct kernels
+    L = 1 << (n + taps - 1).bit_length()
+    X = torch.fft.rfft(data.view(ntrials, n), n=L)
+
+    def fir(hh):
+        y = torch.fft.irfft(X * torch.fft.rfft(hh, n=L), n=L)
+        return y[:, taps // 2: taps // 2 + n].contiguous().view(-1)
+
+    def step():
+        y = fir(h)
+        s = ds.snrs(y)
+        best = torch.full((ntrials,), -1e30, device=data.device).scatter_reduce(
+            0, trial_of_row, s.max(dim=1).values, reduce="amax")
+        return best[inj].mean() - best[~inj].mean()
+
+    def search_only():
+        y = data.detach().clone().requires_grad_(True)
+        s = ds.snrs(y)
+        best = torch.full((ntrials,), -1e30, device=data.device).scatter_reduce(
+            0, trial_of_row, s.max(dim=1).values, reduce="amax")
+        return best[inj].mean() - best[~inj].mean()
+
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    res = {}
+    for name, fn in (("step", step), ("search", search_only)):
+        fw = bw = 0.0
+        for it in range(warmup + steps):
+            h.grad = None
+            torch.cuda.synchronize()
+            e[0].record()
+            loss = fn()
+            e[1].record()
+            (-loss).backward()
+            e[2].record()
+            torch.cuda.synchronize()
+            if it >= warmup:
+                fw += e[0].elapsed_time(e[1])
+                bw += e[1].elapsed_time(e[2])
+        res[name] = (fw / steps, bw / steps, float(loss.detach()),
+                     float(h.grad.norm()) if h.grad is not None else None)
+    ds.close()
+    return {"workload": cfg["name"], "trials": ntrials,
+            "step_forward_ms": res["step"][0], "step_backward_ms": res["step"][1],
+            "search_forward_ms": res["search"][0], "search_backward_ms": res["search"][1],
+            "search_backward_over_forward": res["search"][1] / res["search"][0],
+            "loss": res["step"][2], "fir_grad_norm": res["step"][3]}
+
+
+if __name__ == "__main__":
+    import json
+    import sys
+
+    print(json.dumps(_bench_config4(*[int(a) for a in sys.argv[1:]])))

@@ -23,6 +23,10 @@ CONFIGS = {
             tsamp=64e-6,
             search=dict(period_min=0.2, period_max=30.0, bins_min=240, bins_max=260,
                         ducy_max=0.2, wtsp=1.5, rmed_width=4.0, rmed_minpts=101)),
+    4: dict(name="c4 differentiable 64 x 2^20 samp, 100 us, P 0.5-5 s, b240-260, 257-tap FIR",
+            tsamp=1e-4,
+            search=dict(period_min=0.5, period_max=5.0, bins_min=240, bins_max=260,
+                        ducy_max=0.2, wtsp=1.5, rmed_width=4.0, rmed_minpts=101)),
     5: dict(name="c5 batched 1024 x U[0.85, 1.0]*2^23 samp, 64 us, P 0.2-60 s, b480-520",
             tsamp=64e-6,
             search=dict(period_min=0.2, period_max=60.0, bins_min=480, bins_max=520,
@@ -39,7 +43,7 @@ def trial_lengths(config_id, ntrials, first_index=0):
     out = []
     for i in range(first_index, first_index + ntrials):
         rng = np.random.default_rng(trial_seed(config_id, i) + 7919)
-        if config_id == 1:
+        if config_id in (1, 4):
             out.append(1 << 20)
         elif config_id == 2:
             out.append(1 << 23)
@@ -95,6 +99,9 @@ def make_trial(config_id, index, n, tsamp, device="cuda"):
     elif config_id == 2:
         pulsars = [(0.25, 0.01, 8.0 + 17.0 * rng.random()), (3.7, 0.04, 8.0 + 17.0 * rng.random()),
                    (41.0, 0.08, 8.0 + 17.0 * rng.random())]
+    elif config_id == 4 and index % 2 == 0:  # half the series carry a pulsar
+        pulsars = [(math.exp(rng.uniform(math.log(0.5), math.log(5.0))),
+                    rng.uniform(0.01, 0.05), rng.uniform(8.0, 20.0))]
     elif config_id == 3 and rng.random() < 0.30:
         pulsars = [(math.exp(rng.uniform(math.log(0.2), math.log(30.0))),
                     rng.uniform(0.005, 0.10), rng.uniform(6.0, 30.0))]

@@ -308,3 +308,33 @@ def test_search_gradient_batched_trials(G):
         assert torch.allclose(x1.grad, xb.grad[a:e], rtol=1e-5, atol=1e-6)
         d1.close()
     dsb.close()
+
+
+def test_sparse_row_backward_matches_per_transform(G):
+    # the batched sparse-row backward (rows recomputed from the run's downsampled series)
+    # and the per-transform path (FFA outputs recomputed with rt_ffa2) give the same gradient
+    # with respect to the searched series, to float32 rounding (1e-4 relative L2)
+    import torch
+
+    lens = [1 << 13, 9000, 1 << 13]
+    x = torch.from_numpy(np.concatenate([_series(n, 40 + i) for i, n in enumerate(lens)])).cuda()
+    ds = G.DifferentiableSearch(lens, TSAMP, **KW)
+    (p, fb, s), (z, std, run) = ds.forward(x, keep=True)
+    rng = np.random.default_rng(2)
+    g = torch.zeros_like(s)
+    rows = rng.choice(s.shape[0], 40, replace=False)
+    g[rows] = torch.from_numpy(rng.standard_normal((40, s.shape[1])).astype(np.float32)).cuda()
+    from riptide_b200 import _lib, libcpp
+
+    gz = torch.empty_like(x)
+    _lib.check(_lib.load().rt_search_backward_rows(ds.bs._plan, libcpp._ptr(z), libcpp._ptr(g),
+                                                   libcpp._ptr(gz), 1 << 16, libcpp._stream()))
+    ref = ds._gz_per_transform(x, g, z)
+    err = float((gz - ref).norm() / ref.norm())
+    assert err < 1e-4, err
+    # more rows than allowed: a clear error, nothing written past the limit
+    with pytest.raises(ValueError):
+        _lib.check(_lib.load().rt_search_backward_rows(ds.bs._plan, libcpp._ptr(z),
+                                                       libcpp._ptr(g), libcpp._ptr(gz), 8,
+                                                       libcpp._stream()))
+    ds.close()
