@@ -308,3 +308,24 @@ def test_batched_graph_replay(rb):
     for a, b in zip(outs2, ref):
         assert torch.equal(a, b)
     bs.close()
+
+
+@pytest.mark.parametrize("bmin,bmax,ducy,pmax", [
+    (480, 520, 0.2, 8.0),    # the large batched configuration's bins (12 widths, 16-thread S/N)
+    (100, 110, 0.2, 4.0),    # bins outside the unrolled ranges (generic level loops)
+    (300, 320, 0.3, 6.0),    # more widths than the 10-width register window (generic widths)
+])
+def test_batched_engine_other_bins(rb, bmin, bmax, ducy, pmax):
+    # the persistent engine at bins and width sets other than the default, against the oracle
+    # (C restatement) on the same dereddened + normalised series
+    rng = np.random.default_rng(bmin)
+    n = 1 << 21
+    x = rb.generate_signal(n, 0.61 / 64e-6, ducy=0.02, amplitude=20.0, rng=rng).astype(np.float32)
+    kw = dict(period_min=0.2, period_max=pmax, bins_min=bmin, bins_max=bmax, ducy_max=ducy)
+    bs = rb.BatchedSearch([n], 64e-6, **kw)
+    pgs, zs = bs.search([x], return_normalised=True)
+    z, widths, p, fb, sn = O.ffa_search(x, 64e-6, **kw)
+    assert np.array_equal(pgs[0].widths, widths)
+    assert np.allclose(zs[0], z, rtol=1e-5, atol=1e-5)
+    _check_pgram(pgs[0].periods, pgs[0].foldbins, pgs[0].snrs, p, fb, sn, rtol=1e-4, atol=1e-4)
+    bs.close()
