@@ -224,8 +224,13 @@ def bench_ours(args):
     pool = cpu_pool(ncores) if do_cpu else None
 
     data, lengths, infos = synth.make_batch(args.config, ntrials, first_index=rank * ntrials)
+    tuning = None
+    if args.autotune:  # engine tile choices timed on a sample of this workload
+        from riptide_b200 import tuning as TU
+
+        tuning = TU.autotune(lengths, cfg["tsamp"], sample_trials=16, **cfg["search"])
     t0 = time.perf_counter()
-    bs = rb.BatchedSearch(lengths, cfg["tsamp"], **cfg["search"])
+    bs = rb.BatchedSearch(lengths, cfg["tsamp"], tuning=tuning, **cfg["search"])
     plan_ms = (time.perf_counter() - t0) * 1e3
     st = bs.stats
     nw = int(bs.widths.size)
@@ -348,7 +353,7 @@ def bench_ours(args):
                        "samples_per_gpu": int(sum(lengths)), "periodogram_rows_per_gpu": L,
                        "widths": nw, "l2": "inputs larger than L2 (%.1f GB per step)" %
                        (4 * sum(lengths) / 1e9),
-                       "plan_ms": plan_ms, "stage_ms": {"deredden_normalise": stage[0] / args.steps,
+                       "plan_ms": plan_ms, "tuning": tuning or "default", "stage_ms": {"deredden_normalise": stage[0] / args.steps,
                                                         "downsample": stage[1] / args.steps,
                                                         "ffa_snr": k_ms},
                        "alg_bytes_per_step": bytes_job,
@@ -384,6 +389,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--chunk-trials", type=int, default=32)
     ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()

@@ -42,6 +42,7 @@ SIGNATURES = {
     "rt_periodogram_plain": (ctypes.c_int, [_vp, _sz, _d, _u64p, _sz, _d, _d, _sz, _sz, _vp, _vp, _vp, _vp]),
     "rt_search_plan_create": (ctypes.c_int, [_u64p, _sz, _vp, _u64p, _sz, ctypes.POINTER(_vp)]),
     "rt_search_plan_rows": (ctypes.c_int, [_vp, _u64p]),
+    "rt_search_plan_create_tuned": (ctypes.c_int, [_u64p, _sz, _vp, _u64p, _sz, _vp, ctypes.POINTER(_vp)]),
     "rt_search_plan_stats": (ctypes.c_int, [_vp, _vp]),
     "rt_search_run": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "rt_search_check": (ctypes.c_int, [_vp, _vp]),
@@ -88,6 +89,11 @@ class PlanStats(ctypes.Structure):
         "num_trials", "num_cycles", "num_transforms", "num_work_items", "num_multistage",
         "total_rows", "total_samples", "downsampled_samples", "folded_samples",
         "scrunch_factor")]
+
+
+class SearchTuning(ctypes.Structure):
+    _fields_ = [("rows_fraction", ctypes.c_double), ("snr_threads", ctypes.c_int),
+                ("lag_items", ctypes.c_int)]
 
 
 class SearchTransform(ctypes.Structure):

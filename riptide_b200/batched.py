@@ -18,7 +18,9 @@ class BatchedSearch(object):
 
     def __init__(self, lengths, tsamp, period_min=1.0, period_max=30.0, bins_min=240,
                  bins_max=260, ducy_max=0.20, wtsp=1.5, deredden=True, rmed_width=4.0,
-                 rmed_minpts=101, already_normalised=False, widths=None):
+                 rmed_minpts=101, already_normalised=False, widths=None, tuning=None):
+        """`tuning`: engine tile choices, a dict with any of rows_fraction, snr_threads,
+        lag_items (riptide_b200.tuning.autotune picks them); results do not depend on it."""
         self.lengths = np.ascontiguousarray(np.asarray(lengths, dtype=np.uint64).ravel())
         self.tsamp = float(tsamp)
         self.widths = (np.asarray(widths) if widths is not None
@@ -32,8 +34,17 @@ class BatchedSearch(object):
         w, wp = _lib.u64_array(self.widths)
         lp = self.lengths.ctypes.data_as(_lib._u64p)
         h = ctypes.c_void_p()
-        _lib.check(_lib.load().rt_search_plan_create(lp, self.lengths.size, ctypes.byref(cfg), wp,
-                                                     w.size, ctypes.byref(h)))
+        self.tuning = dict(tuning) if tuning else None
+        if tuning:
+            tn = _lib.SearchTuning(rows_fraction=float(tuning.get("rows_fraction", 0.0)),
+                                   snr_threads=int(tuning.get("snr_threads", 0)),
+                                   lag_items=int(tuning.get("lag_items", 0)))
+            _lib.check(_lib.load().rt_search_plan_create_tuned(
+                lp, self.lengths.size, ctypes.byref(cfg), wp, w.size, ctypes.byref(tn),
+                ctypes.byref(h)))
+        else:
+            _lib.check(_lib.load().rt_search_plan_create(lp, self.lengths.size, ctypes.byref(cfg),
+                                                         wp, w.size, ctypes.byref(h)))
         self._plan = h
         rows = np.zeros(self.lengths.size + 1, dtype=np.uint64)
         _lib.check(_lib.load().rt_search_plan_rows(h, rows.ctypes.data_as(_lib._u64p)))

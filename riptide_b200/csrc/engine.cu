@@ -36,7 +36,7 @@ struct XformRec {
     int plan;                    // index into the stage-plan table
     int seq;                     // multi-stage sequence number, -1 for single-stage transforms
     int src_norm;                // 1: src is in the normalised series arena, 0: downsampled arena
-    int pad;
+    int tune;                    // rows per job (low 16 bits), S/N threads per profile (high)
 };
 
 struct WorkItem {
@@ -210,7 +210,7 @@ __device__ void sched_decode(const EngineArgs& A, long long t, SchedItem& it)
     L.stage = stage;
     L.last = stage == P.nstages - 1;
     L.jobs_of_stage = P.jobs[stage];
-    L.cap_rows = engine_cap_rows(X.b);
+    L.cap_rows = X.tune & 0xffff;
     it.dep = nullptr;
     it.target = 0;
     if (J.hi > J.lo && X.seq >= 0) {
@@ -435,7 +435,7 @@ __global__ void __launch_bounds__(kEngineThreads, 1) k_search_persistent(EngineA
                 }
                 mark(kPhLevels);
                 if (last) {
-                    if (snr_tpr(b) == 8)
+                    if ((X.tune >> 16) == 8)
                         final_stage_outputs<8>(T, X, A, S, Lay.buf0, Lay.buf1, fstride, cap_rows);
                     else
                         final_stage_outputs<16>(T, X, A, S, Lay.buf0, Lay.buf1, fstride, cap_rows);
@@ -728,6 +728,7 @@ __global__ void k_normalise(const float* __restrict__ x, TrialArrays A, const do
 struct SearchPlan {
     // configuration
     rt_search_config cfg;
+    rt_search_tuning tuning = {1.0, 0, 0};
     std::vector<int> widths;
     int nfast = 0;
     std::vector<size_t> lengths, offsets;
@@ -833,6 +834,7 @@ static int plan_build(SearchPlan& P)
     P.out_rows_off.assign(T + 1, 0);
     P.ds_off.assign((size_t)T * C, 0);
     std::map<std::pair<int, long long>, int> plan_index;
+    const size_t lag_items = P.tuning.lag_items > 0 ? (size_t)P.tuning.lag_items : kLagItems;
     std::set<std::tuple<size_t, int, int>> deferred;  // (due item count, xform, stage)
     std::vector<int> seq_xform;                        // xform of each multi-stage sequence
     std::vector<std::tuple<size_t, int, int>> seq_pending;  // its deferred entry, if any
@@ -844,7 +846,7 @@ static int plan_build(SearchPlan& P)
         const int seq = P.xforms[xi].seq;
         if (seq >= 0) {
             if (stage + 1 < sp.nstages) {
-                auto e = std::make_tuple(P.items.size() + kLagItems, xi, stage + 1);
+                auto e = std::make_tuple(P.items.size() + lag_items, xi, stage + 1);
                 deferred.insert(e);
                 seq_pending[seq] = e;
                 seq_has_pending[seq] = 1;
@@ -889,7 +891,11 @@ static int plan_build(SearchPlan& P)
                 if (re == 0) continue;
                 if (rows >= (1u << 24))
                     return set_error(RT_EINVAL, "transform of %zu rows is too large", rows);
-                const int capr = engine_cap_rows((int)b);
+                // rows per job: the shared-memory capacity, scaled by the tuning
+                const double frac = P.tuning.rows_fraction > 0 ? std::min(1.0, P.tuning.rows_fraction) : 1.0;
+                const int capr = std::max(4, (int)((double)engine_cap_rows((int)b) * frac));
+                // S/N threads per profile: 8 where the register window allows it, unless tuned
+                const int tpr = (P.tuning.snr_threads == 16) ? 16 : snr_tpr((int)b);
                 const auto key = std::make_pair((int)rows, (long long)re * 8192 + (long long)b);
                 int pi;
                 auto itp = plan_index.find(key);
@@ -916,6 +922,7 @@ static int plan_build(SearchPlan& P)
                 X.stdnoise = (float)sqrt((double)rows * downsampled_variance(N, f));
                 X.plan = pi;
                 X.seq = -1;
+                X.tune = capr | (tpr << 16);
                 const int xi = (int)P.xforms.size();
                 if (multi) {
                     X.seq = P.nseq++;
@@ -1510,9 +1517,9 @@ struct rt_search_plan {
     SearchPlan p;
 };
 
-extern "C" int rt_search_plan_create(const uint64_t* lengths, size_t ntrials,
-                                     const rt_search_config* cfg, const uint64_t* widths,
-                                     size_t num_widths, rt_search_plan** out)
+static int plan_create(const uint64_t* lengths, size_t ntrials, const rt_search_config* cfg,
+                       const uint64_t* widths, size_t num_widths,
+                       const rt_search_tuning* tuning, rt_search_plan** out)
 {
     if (!out || !cfg || (!lengths && ntrials) || (!widths && num_widths))
         return set_error(RT_EINVAL, "null argument");
@@ -1524,6 +1531,7 @@ extern "C" int rt_search_plan_create(const uint64_t* lengths, size_t ntrials,
     if (!h) return set_error(RT_ENOMEM, "out of host memory");
     SearchPlan& P = h->p;
     P.cfg = *cfg;
+    if (tuning) P.tuning = *tuning;
     for (size_t i = 0; i < num_widths; ++i) {
         // snr.hpp:21-31
         if (!(widths[i] > 0 && widths[i] < cfg->bins_min)) {
@@ -1551,6 +1559,26 @@ extern "C" int rt_search_plan_create(const uint64_t* lengths, size_t ntrials,
     }
     *out = h;
     return RT_OK;
+}
+
+extern "C" int rt_search_plan_create(const uint64_t* lengths, size_t ntrials,
+                                     const rt_search_config* cfg, const uint64_t* widths,
+                                     size_t num_widths, rt_search_plan** out)
+{
+    return plan_create(lengths, ntrials, cfg, widths, num_widths, nullptr, out);
+}
+
+extern "C" int rt_search_plan_create_tuned(const uint64_t* lengths, size_t ntrials,
+                                           const rt_search_config* cfg, const uint64_t* widths,
+                                           size_t num_widths, const rt_search_tuning* tuning,
+                                           rt_search_plan** out)
+{
+    if (tuning && !(tuning->rows_fraction >= 0.0 && tuning->rows_fraction <= 1.0))
+        return set_error(RT_EINVAL, "rows_fraction must be in [0, 1]");
+    if (tuning && tuning->snr_threads != 0 && tuning->snr_threads != 8 && tuning->snr_threads != 16)
+        return set_error(RT_EINVAL, "snr_threads must be 0, 8 or 16");
+    if (tuning && tuning->lag_items < 0) return set_error(RT_EINVAL, "lag_items must be >= 0");
+    return plan_create(lengths, ntrials, cfg, widths, num_widths, tuning, out);
 }
 
 extern "C" int rt_search_plan_rows(const rt_search_plan* plan, uint64_t* row_offsets)

@@ -81,3 +81,23 @@ def test_batched_plan_errors():
     with pytest.raises(ValueError, match="Downsampling factor"):
         # the last octave needs f > size
         BatchedSearch([200], 1e-3, period_min=0.24, period_max=60.0, deredden=False)
+
+
+def test_tuned_plan_checks_and_shapes():
+    # tuning changes the work split only: same periodogram rows; invalid values are rejected
+    from riptide_b200 import BatchedSearch
+
+    kw = dict(period_min=0.2, period_max=30.0)
+    base = BatchedSearch([2 ** 22], 64e-6, **kw)
+    tuned = BatchedSearch([2 ** 22], 64e-6, tuning={"rows_fraction": 0.7, "snr_threads": 16,
+                                                     "lag_items": 100}, **kw)
+    try:
+        assert np.array_equal(base.row_offsets, tuned.row_offsets)
+        assert tuned.stats["num_transforms"] == base.stats["num_transforms"]
+        assert tuned.stats["num_work_items"] > base.stats["num_work_items"]  # smaller jobs
+    finally:
+        base.close()
+        tuned.close()
+    for bad in ({"rows_fraction": 1.5}, {"snr_threads": 12}, {"lag_items": -1}):
+        with pytest.raises(ValueError):
+            BatchedSearch([100000], 1e-3, period_min=0.5, period_max=2.0, tuning=bad)

@@ -329,3 +329,28 @@ def test_batched_engine_other_bins(rb, bmin, bmax, ducy, pmax):
     assert np.allclose(zs[0], z, rtol=1e-5, atol=1e-5)
     _check_pgram(pgs[0].periods, pgs[0].foldbins, pgs[0].snrs, p, fb, sn, rtol=1e-4, atol=1e-4)
     bs.close()
+
+
+def test_tuned_engine_is_bit_identical(rb):
+    # the tile choices change the work split, never the periodogram; the autotuner returns
+    # one of its candidates
+    import torch
+
+    from riptide_b200 import tuning as TU
+
+    rng = np.random.default_rng(81)
+    lengths = [300001, 262144, 280000]
+    x = torch.from_numpy(np.concatenate([rng.standard_normal(n).astype(np.float32)
+                                         for n in lengths])).cuda()
+    kw = dict(period_min=0.2, period_max=8.0, bins_min=240, bins_max=260)
+    ref = [t.clone() for t in rb.BatchedSearch(lengths, 64e-6, **kw).run(x)]
+    for tun in ({"rows_fraction": 0.6}, {"snr_threads": 16}, {"lag_items": 64},
+                {"rows_fraction": 0.8, "snr_threads": 16, "lag_items": 2000}):
+        bs = rb.BatchedSearch(lengths, 64e-6, tuning=tun, **kw)
+        out = bs.run(x)
+        for a, b in zip(out, ref):
+            assert torch.equal(a, b), tun
+        bs.close()
+    best = TU.autotune(lengths, 64e-6, sample_trials=2, repeats=1, **kw)
+    assert best in TU.candidates(260)
+    assert TU.autotune(lengths, 64e-6, sample_trials=2, repeats=1, **kw) == best  # cached
