@@ -260,3 +260,68 @@ def ffa_search(data, tsamp, period_min=1.0, period_max=30.0, fpmin=8, bins_min=2
         periods, foldbins, snrs = libcpp.periodogram(
             data, tsamp, widths.astype(np.uint64), period_min, period_max, bins_min, bins_max)
     return data, widths, periods, foldbins, snrs
+
+
+# ------------------------------------------------------------------------------------------
+# Peak detection (peak_detection.py:38-240, clustering.py:4-48)
+# ------------------------------------------------------------------------------------------
+def cluster1d(x, r, already_sorted=False):
+    """clustering.py:4-48: friends-of-friends in 1D, clusters as arrays of indices."""
+    if not len(x):
+        return []
+    if not already_sorted:
+        indices = x.argsort()
+        diff = np.diff(x[indices])
+    else:
+        indices = np.arange(len(x))
+        diff = np.diff(x)
+    ibreaks = np.where(abs(diff) > r)[0]
+    if not len(ibreaks):
+        return [indices]
+    ibounds = np.concatenate(([0], ibreaks + 1, [len(x)]))
+    return [indices[a:b] for a, b in zip(ibounds[:-1], ibounds[1:])]
+
+
+def segment_stats(f, s, T, segwidth=5.0):
+    """peak_detection.py:38-86: centre frequency, median S/N and IQR-based S/N deviation of
+    consecutive segments of `segwidth / T` Hz."""
+    import math
+
+    w = segwidth / T
+    m = math.ceil(abs(f[-1] - f[0]) / w)
+    p = len(f) // m
+    n = m * p
+    fc = np.median(f[:n].reshape(m, p), axis=1)
+    s25, smed, s75 = np.percentile(s[:n].reshape(m, p), (25, 50, 75), axis=-1)
+    return fc, smed, (s75 - s25) / 1.349
+
+
+def find_peaks(periods, foldbins, snrs, widths, tobs, dm=None, smin=6.0, segwidth=5.0,
+               nstd=6.0, minseg=10, polydeg=2, clrad=0.1):
+    """peak_detection.py:112-240 on periodogram arrays. Returns (peaks, polycos): peaks as
+    tuples (period, freq, width, ducy, iw, ip, snr, dm) sorted by decreasing S/N, polycos as
+    {iw: coefficient list}."""
+    f = 1.0 / periods
+    T = tobs
+    peaks, polycos = [], {}
+    for iw, width in enumerate(widths):
+        s = snrs[:, iw].astype(float)
+        fc, smed, sstd = segment_stats(f, s, T, segwidth=segwidth)
+        sc = smed + nstd * sstd
+        if len(fc) >= minseg:
+            poly = np.poly1d(np.polyfit(np.log(fc), sc, polydeg))
+            polyco = poly.coefficients
+        else:
+            polyco = [smin]
+            poly = np.poly1d(polyco)
+        dynthr = poly(np.log(f))
+        indices = np.where((s > dynthr) & (s > smin))[0]
+        for cl in cluster1d(f[indices], clrad / T):
+            ix = indices[cl]
+            ip = ix[s[ix].argmax()]
+            pf = f[ip]
+            peaks.append((float(1.0 / pf), float(pf), int(width), float(width) / foldbins[ip],
+                          int(iw), int(ip), float(s[ip]), dm))
+        polycos[iw] = polyco
+    peaks = sorted(peaks, key=lambda p: p[6], reverse=True)
+    return peaks, polycos

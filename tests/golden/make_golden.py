@@ -72,8 +72,10 @@ def import_reference():
     import importlib
 
     mods = {}
-    for name in ("timing", "ffautils", "libffa", "running_medians", "time_series", "search"):
+    for name in ("timing", "ffautils", "libffa", "running_medians", "time_series", "search",
+                 "clustering", "peak_detection"):
         mods[name] = importlib.import_module("riptide." + name)
+    mods["periodogram"] = importlib.import_module("riptide.periodogram")
     return libcpp, mods
 
 
@@ -188,6 +190,40 @@ def main():
     g["frm_w2001_m101"] = M["running_medians"].fast_running_median(x, 2001, 101)
     g["frm_w37_m41"] = M["running_medians"].fast_running_median(x, 37, 41)
     np.savez_compressed(os.path.join(HERE, "glue.npz"), **g)
+
+    # --- find_peaks on the periodograms above and one longer search --------------------
+    fp = {}
+    pgrams = []
+    for i, (nsamp, tsamp, period, amp, kw) in enumerate(cases):
+        pgrams.append((fs[f"p{i}"], fs[f"fb{i}"], fs[f"s{i}"], fs[f"w{i}"], nsamp * tsamp))
+    crng = np.random.default_rng(4242)
+    nsamp, tsamp = 1 << 15, 2e-3
+    t = np.arange(nsamp) * tsamp
+    data = crng.standard_normal(nsamp)
+    for per, amp in ((0.731, 1.2), (2.9, 0.9)):
+        data += amp * np.exp(-0.5 * ((np.mod(t, per) - per / 2) / (0.01 * per)) ** 2)
+    tsdr, pgram = ffa_search(TS(data.astype(np.float32), tsamp), period_min=0.5, period_max=5.0)
+    pgrams.append((pgram.periods, pgram.foldbins, pgram.snrs, np.asarray(pgram.widths),
+                   nsamp * tsamp))
+    Pg = M["periodogram"].Periodogram
+    for i, (p, fb, s, w, tobs) in enumerate(pgrams):
+        pg = Pg(w, p, fb, s, metadata={"tobs": tobs, "dm": None})
+        peaks, polycos = M["peak_detection"].find_peaks(pg)
+        if i >= len(cases):  # the first periodograms are those of ffa_search.npz
+            fp[f"p{i}"], fp[f"fb{i}"], fp[f"s{i}"], fp[f"w{i}"] = p, fb, s, w
+        fp[f"tobs{i}"] = np.float64(tobs)
+        fp[f"ip{i}"] = np.array([k.ip for k in peaks], dtype=np.int64)
+        fp[f"iw{i}"] = np.array([k.iw for k in peaks], dtype=np.int64)
+        fp[f"snr{i}"] = np.array([k.snr for k in peaks], dtype=np.float64)
+        fp[f"freq{i}"] = np.array([k.freq for k in peaks], dtype=np.float64)
+        fp[f"ducy{i}"] = np.array([k.ducy for k in peaks], dtype=np.float64)
+        deg = max(len(v) for v in polycos.values())
+        pc = np.full((len(w), deg), np.nan)
+        for iw, v in polycos.items():
+            pc[iw, :len(v)] = v
+        fp[f"polycos{i}"] = pc
+    np.savez_compressed(os.path.join(HERE, "find_peaks.npz"), **fp, n=len(pgrams),
+                        n_from_ffa_search=len(cases))
 
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):

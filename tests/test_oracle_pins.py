@@ -160,3 +160,38 @@ def test_oracle_matches_built_reference_random():
     w = O.generate_width_trials(240)
     x = rng.standard_normal((400, 257)).astype(np.float32) * 3
     assert np.array_equal(O.C().snr2(x, w, 2.5), R.snr2(x, w.astype(np.uint64), 2.5))
+
+
+def _find_peaks_cases(golden):
+    """(periods, foldbins, snrs, widths, tobs, expected) of every find_peaks golden case."""
+    g = golden("find_peaks.npz")
+    fs = golden("ffa_search.npz")
+    out = []
+    for i in range(int(g["n"])):
+        if i < int(g["n_from_ffa_search"]):
+            p, fb, s, w = fs[f"p{i}"], fs[f"fb{i}"], fs[f"s{i}"], fs[f"w{i}"]
+        else:
+            p, fb, s, w = g[f"p{i}"], g[f"fb{i}"], g[f"s{i}"], g[f"w{i}"]
+        exp = {k: g[f"{k}{i}"] for k in ("ip", "iw", "snr", "freq", "ducy", "polycos")}
+        out.append((p, fb, s, w, float(g[f"tobs{i}"]), exp))
+    return out
+
+
+def test_find_peaks_golden(golden):
+    # the numpy restatement against the reference's own find_peaks (peak_detection.py)
+    for p, fb, s, w, tobs, exp in _find_peaks_cases(golden):
+        peaks, polycos = O.find_peaks(p, fb, s, w, tobs)
+        assert [k[5] for k in peaks] == list(exp["ip"])
+        assert [k[4] for k in peaks] == list(exp["iw"])
+        assert np.array_equal([k[6] for k in peaks], exp["snr"])
+        assert np.array_equal([k[1] for k in peaks], exp["freq"])
+        assert np.array_equal([k[3] for k in peaks], exp["ducy"])
+        for iw, c in polycos.items():
+            ref = exp["polycos"][iw]
+            assert np.array_equal(np.asarray(c), ref[~np.isnan(ref)])
+
+
+def test_cluster1d_known_answers():
+    assert O.cluster1d(np.array([]), 1.0) == []
+    cl = O.cluster1d(np.array([5.0, 1.0, 1.5, 9.0, 4.6]), 0.6)
+    assert [list(c) for c in cl] == [[1, 2], [4, 0], [3]]
