@@ -248,6 +248,28 @@ int rt_search_pipeline_check(rt_search_pipeline* pipeline, void* stream);
 void rt_search_pipeline_destroy(rt_search_pipeline* pipeline);
 
 /* ---------------------------------------------------------------------------------
+ * Peak detection (peak_detection.py:38-146): the device parts of find_peaks for a batch of
+ * periodograms packed by trial (h_row_offsets: ntrials + 1 entries).
+ * -------------------------------------------------------------------------------*/
+/* Segment statistics of segment_stats (peak_detection.py:38-86): per trial the frequency
+ * range is cut into m = ceil(|f[-1] - f[0]| T / segwidth) segments of p = rows // m points;
+ * h_seg_offsets (ntrials + 1, output) gives each trial's first segment. With d_fc and d_sc
+ * given: d_fc[seg] = median frequency, d_sc[seg * num_widths + iw] = median S/N + nstd *
+ * IQR / 1.349 (np.median / np.percentile 'linear'). At most 4096 points per segment. */
+int rt_peak_segments(const double* d_periods, const float* d_snrs, size_t num_widths,
+                     const uint64_t* h_row_offsets, size_t ntrials, const double* h_tobs,
+                     double segwidth, double nstd, uint64_t* h_seg_offsets, double* d_fc,
+                     double* d_sc, void* stream);
+/* Points whose S/N exceeds both smin and the polynomial threshold in log f (coefficients
+ * d_coef[(trial * num_widths + iw) * num_coef + k], highest power first, evaluated as
+ * np.polyval), listed in d_sel as row * num_widths + iw in no particular order; *h_count =
+ * their number (RT_EINVAL when above `capacity`). Synchronises `stream`. */
+int rt_peak_select(const double* d_periods, const float* d_snrs, size_t num_widths,
+                   const uint64_t* h_row_offsets, size_t ntrials, const double* d_coef,
+                   size_t num_coef, double smin, uint64_t* d_sel, size_t capacity,
+                   size_t* h_count, void* stream);
+
+/* ---------------------------------------------------------------------------------
  * Adjoints of the search steps, for gradients of a loss of the periodogram with respect to
  * the searched series (differentiable search; no counterpart in the reference, whose search
  * is not differentiable). Each computes the transpose of the Jacobian of the forward step

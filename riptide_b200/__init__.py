@@ -7,6 +7,7 @@ from . import libcpp
 from .batched import BatchedSearch, SearchPipeline, ffa_search_batched
 from .ffautils import generate_width_trials
 from .libffa import boxcar_snr, downsample, ffa1, ffa2, ffafreq, ffaprd, generate_signal
+from .peaks import Peak, find_peaks, find_peaks_batched
 from .periodogram import Periodogram
 from .running_medians import fast_running_median, running_median
 from .search import ffa_search
@@ -17,4 +18,5 @@ __all__ = [
     "ffa1",
     "ffa2", "ffafreq", "ffaprd", "generate_signal", "downsample", "boxcar_snr",
     "running_median", "fast_running_median", "generate_width_trials", "libcpp",
+    "find_peaks", "find_peaks_batched", "Peak",
 ]

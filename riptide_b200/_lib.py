@@ -55,6 +55,8 @@ SIGNATURES = {
     "rt_search_plan_transforms": (ctypes.c_int, [_vp, _vp]),
     "rt_search_normalisation": (ctypes.c_int, [_vp, ctypes.POINTER(_d), ctypes.POINTER(_d), _vp]),
     "rt_search_backward_rows": (ctypes.c_int, [_vp, _vp, _vp, _vp, _sz, _vp]),
+    "rt_peak_segments": (ctypes.c_int, [_vp, _vp, _sz, _u64p, _sz, ctypes.POINTER(_d), _d, _d, _u64p, _vp, _vp, _vp]),
+    "rt_peak_select": (ctypes.c_int, [_vp, _vp, _sz, _u64p, _sz, _vp, _sz, _d, _vp, _sz, ctypes.POINTER(_sz), _vp]),
     "rt_snr2_backward": (ctypes.c_int, [_vp, _sz, _sz, _u64p, _sz, ctypes.c_float, _vp, _vp, _vp]),
     "rt_ffa2_transpose": (ctypes.c_int, [_vp, _sz, _sz, _vp, _vp]),
     "rt_downsample_adjoint": (ctypes.c_int, [_vp, _sz, _d, _vp, _vp]),

@@ -1,0 +1,235 @@
+// Peak detection on the device (peak_detection.py:38-240 of the reference): the per-segment
+// S/N statistics that the dynamic threshold is fitted to, and the selection of the
+// periodogram points above that threshold, for every (trial, width) of a batch of
+// periodograms at once. The threshold fit itself (a degree-2 polynomial in log f over a few
+// hundred control points) and the clustering of the selected points run on the host, in the
+// reference's own numpy calls (riptide_b200/peaks.py).
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+
+namespace rt {
+
+constexpr int kSegThreads = 256;
+constexpr int kSegMaxPoints = 4096;  // points per segment sorted in shared memory
+
+// In-place ascending bitonic sort of n (power of two) doubles in shared memory.
+__device__ void bitonic_sort(double* a, int n)
+{
+    for (int k = 2; k <= n; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const bool up = (i & k) == 0;
+                    const double x = a[i], y = a[l];
+                    if ((x > y) == up) {
+                        a[i] = y;
+                        a[l] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// numpy's linear interpolation between two order statistics (numpy _lerp)
+__device__ __forceinline__ double np_lerp(double a, double b, double t)
+{
+    const double d = __dsub_rn(b, a);
+    return (t >= 0.5) ? __dsub_rn(b, __dmul_rn(d, __dsub_rn(1.0, t))) : __dadd_rn(a, __dmul_rn(d, t));
+}
+
+// np.percentile(x, q) of n sorted values, method 'linear'
+__device__ __forceinline__ double np_percentile_sorted(const double* a, int n, double q)
+{
+    const double v = __dmul_rn((double)(n - 1), q);
+    const double prev = floor(v);
+    const int i0 = (int)prev;
+    const int i1 = min(i0 + 1, n - 1);
+    return np_lerp(a[i0], a[i1], __dsub_rn(v, prev));
+}
+
+struct SegTrial {
+    unsigned long long row0;  // first periodogram row of the trial
+    int seg0, m, p, pad;      // first global segment, segments, points per segment
+};
+
+// One CTA per (segment, width): sc = median + nstd * IQR / 1.349 of the segment's S/N
+// (segment_stats, peak_detection.py:38-86). CTAs of width 0 also write the segment's median
+// frequency fc.
+__global__ void __launch_bounds__(kSegThreads)
+    k_peak_segments(const double* __restrict__ periods, const float* __restrict__ snrs, int nw,
+                    const SegTrial* __restrict__ trials, int ntrials, double nstd,
+                    double* __restrict__ fc, double* __restrict__ sc)
+{
+    __shared__ double v[kSegMaxPoints];
+    const int seg = blockIdx.x, iw = blockIdx.y;
+    int lo = 0, hi = ntrials - 1;  // trial of this segment
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (trials[mid].seg0 <= seg) lo = mid;
+        else hi = mid - 1;
+    }
+    const SegTrial T = trials[lo];
+    const int j = seg - T.seg0, p = T.p;
+    int n2 = 1;
+    while (n2 < p) n2 <<= 1;
+    const size_t r0 = T.row0 + (size_t)j * p;
+    for (int i = threadIdx.x; i < n2; i += blockDim.x)
+        v[i] = (i < p) ? (double)snrs[(r0 + i) * nw + iw] : INFINITY;
+    __syncthreads();
+    bitonic_sort(v, n2);
+    if (threadIdx.x == 0) {
+        const double s25 = np_percentile_sorted(v, p, 0.25);
+        const double s50 = np_percentile_sorted(v, p, 0.5);
+        const double s75 = np_percentile_sorted(v, p, 0.75);
+        const double sstd = __ddiv_rn(__dsub_rn(s75, s25), 1.349);
+        sc[(size_t)seg * nw + iw] = __dadd_rn(s50, __dmul_rn(nstd, sstd));
+    }
+    if (iw != 0) return;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n2; i += blockDim.x)
+        v[i] = (i < p) ? __ddiv_rn(1.0, periods[r0 + i]) : INFINITY;
+    __syncthreads();
+    bitonic_sort(v, n2);
+    if (threadIdx.x == 0)  // np.median: the middle value, or the mean of the middle two
+        fc[seg] = (p & 1) ? v[p / 2] : __ddiv_rn(__dadd_rn(v[p / 2 - 1], v[p / 2]), 2.0);
+}
+
+// Points above the dynamic threshold poly(log f) and above smin (find_peaks_single,
+// peak_detection.py:112-146), as (row * nw + iw), in any order.
+__global__ void k_peak_select(const double* __restrict__ periods, const float* __restrict__ snrs,
+                              int nw, const unsigned long long* __restrict__ row_trial_end,
+                              int ntrials, const double* __restrict__ coef, int ncoef,
+                              double smin, unsigned long long rows,
+                              unsigned long long* __restrict__ sel, unsigned long long cap,
+                              unsigned long long* __restrict__ count)
+{
+    for (unsigned long long e = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+         e < rows * nw; e += (unsigned long long)gridDim.x * blockDim.x) {
+        const unsigned long long r = e / nw;
+        const int iw = (int)(e - r * nw);
+        const double s = (double)snrs[e];
+        if (!(s > smin)) continue;
+        int lo = 0, hi = ntrials - 1;  // first trial whose end is beyond r
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (row_trial_end[mid] > r) hi = mid;
+            else lo = mid + 1;
+        }
+        const double x = log(__ddiv_rn(1.0, periods[r]));
+        const double* c = coef + ((size_t)lo * nw + iw) * ncoef;
+        double y = 0.0;  // np.polyval: y = y * x + c_k, no fused multiply-add
+        for (int k = 0; k < ncoef; ++k) y = __dadd_rn(__dmul_rn(y, x), c[k]);
+        if (s > y) {
+            const unsigned long long slot = atomicAdd(count, 1ull);
+            if (slot < cap) sel[slot] = e;
+        }
+    }
+}
+
+}  // namespace rt
+
+using namespace rt;
+
+extern "C" int rt_peak_segments(const double* d_periods, const float* d_snrs, size_t num_widths,
+                                const uint64_t* h_row_offsets, size_t ntrials,
+                                const double* h_tobs, double segwidth, double nstd,
+                                uint64_t* h_seg_offsets, double* d_fc, double* d_sc, void* stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!d_periods || !h_row_offsets || !h_tobs || !h_seg_offsets)
+        return set_error(RT_EINVAL, "null argument");
+    if (num_widths == 0 || num_widths > 65535) return set_error(RT_EINVAL, "bad number of widths");
+    // segment layout of every trial: m = ceil(|f[-1] - f[0]| / w), p = rows // m
+    std::vector<double> ends(2 * ntrials);
+    for (size_t t = 0; t < ntrials; ++t) {
+        const uint64_t a = h_row_offsets[t], b = h_row_offsets[t + 1];
+        if (b <= a) return set_error(RT_EINVAL, "periodogram %zu is empty", t);
+        RT_TRY_CUDA(cudaMemcpyAsync(&ends[2 * t], d_periods + a, sizeof(double),
+                                    cudaMemcpyDeviceToHost, st));
+        RT_TRY_CUDA(cudaMemcpyAsync(&ends[2 * t + 1], d_periods + b - 1, sizeof(double),
+                                    cudaMemcpyDeviceToHost, st));
+    }
+    RT_TRY_CUDA(cudaStreamSynchronize(st));
+    std::vector<SegTrial> tr(ntrials);
+    uint64_t seg = 0;
+    h_seg_offsets[0] = 0;
+    for (size_t t = 0; t < ntrials; ++t) {
+        const double w = segwidth / h_tobs[t];
+        const double span = std::fabs(1.0 / ends[2 * t + 1] - 1.0 / ends[2 * t]);
+        const double mf = std::ceil(span / w);
+        if (!(mf >= 1.0) || !std::isfinite(mf))
+            return set_error(RT_EINVAL, "periodogram %zu spans no frequency segment", t);
+        const uint64_t rows = h_row_offsets[t + 1] - h_row_offsets[t];
+        const uint64_t m = (uint64_t)mf;
+        const uint64_t p = rows / m;
+        if (p == 0) return set_error(RT_EINVAL, "periodogram %zu has fewer rows than segments", t);
+        if (p > (uint64_t)kSegMaxPoints)
+            return set_error(RT_EINVAL, "segments of %llu points exceed the device limit (%d)",
+                             (unsigned long long)p, kSegMaxPoints);
+        tr[t].row0 = h_row_offsets[t];
+        tr[t].seg0 = (int)seg;
+        tr[t].m = (int)m;
+        tr[t].p = (int)p;
+        tr[t].pad = 0;
+        seg += m;
+        h_seg_offsets[t + 1] = seg;
+    }
+    if (!d_fc || !d_sc) return RT_OK;  // layout only
+    if (!d_snrs) return set_error(RT_EINVAL, "null argument");
+    if (seg >= (1ull << 31)) return set_error(RT_EINVAL, "too many segments");
+    SegTrial* d_tr = nullptr;
+    RT_TRY_CUDA(cudaMallocAsync((void**)&d_tr, ntrials * sizeof(SegTrial), st));
+    int s = check_cuda(cudaMemcpyAsync(d_tr, tr.data(), ntrials * sizeof(SegTrial),
+                                       cudaMemcpyHostToDevice, st), "peak_segments");
+    if (s == RT_OK && seg > 0) {
+        dim3 grid((unsigned)seg, (unsigned)num_widths);
+        k_peak_segments<<<grid, kSegThreads, 0, st>>>(d_periods, d_snrs, (int)num_widths, d_tr,
+                                                      (int)ntrials, nstd, d_fc, d_sc);
+        s = check_cuda(cudaGetLastError(), "peak_segments");
+    }
+    cudaFreeAsync(d_tr, st);
+    return s;
+}
+
+extern "C" int rt_peak_select(const double* d_periods, const float* d_snrs, size_t num_widths,
+                              const uint64_t* h_row_offsets, size_t ntrials, const double* d_coef,
+                              size_t num_coef, double smin, uint64_t* d_sel, size_t capacity,
+                              size_t* h_count, void* stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!d_periods || !d_snrs || !h_row_offsets || !d_coef || !d_sel || !h_count)
+        return set_error(RT_EINVAL, "null argument");
+    if (num_coef == 0 || num_widths == 0) return set_error(RT_EINVAL, "bad coefficient count");
+    const uint64_t rows = h_row_offsets[ntrials];
+    unsigned long long* d_aux = nullptr;  // [ntrials] trial row ends, then the counter
+    RT_TRY_CUDA(cudaMallocAsync((void**)&d_aux, (ntrials + 1) * sizeof(unsigned long long), st));
+    int s = check_cuda(cudaMemcpyAsync(d_aux, h_row_offsets + 1, ntrials * sizeof(uint64_t),
+                                       cudaMemcpyHostToDevice, st), "peak_select");
+    if (s == RT_OK)
+        s = check_cuda(cudaMemsetAsync(d_aux + ntrials, 0, sizeof(unsigned long long), st), "peak_select");
+    if (s == RT_OK && rows > 0) {
+        const size_t work = (size_t)rows * num_widths;
+        const int grid = (int)std::min<size_t>((work + 255) / 256, 148 * 32);
+        k_peak_select<<<grid, 256, 0, st>>>(d_periods, d_snrs, (int)num_widths, d_aux,
+                                            (int)ntrials, d_coef, (int)num_coef, smin, rows,
+                                            (unsigned long long*)d_sel, capacity, d_aux + ntrials);
+        s = check_cuda(cudaGetLastError(), "peak_select");
+    }
+    unsigned long long count = 0;
+    if (s == RT_OK)
+        s = check_cuda(cudaMemcpyAsync(&count, d_aux + ntrials, sizeof(count),
+                                       cudaMemcpyDeviceToHost, st), "peak_select");
+    if (s == RT_OK) s = check_cuda(cudaStreamSynchronize(st), "peak_select");
+    cudaFreeAsync(d_aux, st);
+    if (s != RT_OK) return s;
+    *h_count = (size_t)count;
+    if (count > capacity)
+        return set_error(RT_EINVAL, "%llu points pass the threshold (capacity %zu)", count, capacity);
+    return RT_OK;
+}

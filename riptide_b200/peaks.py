@@ -1,0 +1,150 @@
+"""Peak detection in periodograms (peak_detection.py:38-240 and clustering.py:4-48 of the
+reference), for one periodogram or a whole batch on the device.
+
+Per periodogram and width trial, the reference fits a dynamic S/N threshold: the frequency
+range is cut into segments of segwidth / T_obs Hz, each segment gives a control point
+(median frequency, median S/N + nstd * IQR / 1.349), a degree-`polydeg` polynomial in log f is
+fitted to the control points (a constant `smin` below `minseg` segments), and the points
+above both the threshold and `smin` are clustered in frequency (radius clrad / T_obs), one
+peak per cluster at its highest S/N.
+
+Here the segment statistics (sorts of every segment's S/N and frequencies) and the
+thresholding of every periodogram point run on the GPU (rt_peak_segments, rt_peak_select);
+the polynomial fits (np.polyfit, a few hundred points each) and the clustering of the
+selected points run on the host with the reference's numpy calls, so that the peaks are the
+ones the reference finds.
+"""
+import ctypes
+import typing
+
+import numpy as np
+
+from . import _lib, libcpp
+
+
+class Peak(typing.NamedTuple):
+    """A peak of a periodogram (peak_detection.py:14-35)."""
+
+    period: float
+    freq: float
+    width: int
+    ducy: float
+    iw: int
+    ip: int
+    snr: float
+    dm: float
+
+    def summary_dict(self):
+        attrs = ("period", "freq", "dm", "width", "ducy", "snr")
+        return {a: getattr(self, a) for a in attrs}
+
+
+def _cluster1d(x, r):
+    """Friends-of-friends clusters of 1D points within r (clustering.py:4-48)."""
+    if not len(x):
+        return []
+    indices = x.argsort()
+    ibreaks = np.where(abs(np.diff(x[indices])) > r)[0]
+    if not len(ibreaks):
+        return [indices]
+    ibounds = np.concatenate(([0], ibreaks + 1, [len(x)]))
+    return [indices[a:b] for a, b in zip(ibounds[:-1], ibounds[1:])]
+
+
+def find_peaks_batched(periods, foldbins, snrs, row_offsets, tobs, widths, dms=None,
+                       smin=6.0, segwidth=5.0, nstd=6.0, minseg=10, polydeg=2, clrad=0.1,
+                       capacity=1 << 22):
+    """Peaks of a batch of periodograms packed by trial (as BatchedSearch.run returns them:
+    CUDA tensors periods f64[L], foldbins i32[L], snrs f32[L, nw]; row_offsets[T + 1]).
+    `tobs`: per-trial observation time (s). Returns a list, per trial, of (peaks, polycos)
+    as find_peaks returns them."""
+    torch = libcpp._t()
+    lib = _lib.load()
+    st = libcpp._stream()
+    rows = np.ascontiguousarray(np.asarray(row_offsets, dtype=np.uint64))
+    T = rows.size - 1
+    nw = int(np.asarray(widths).size)
+    tob = np.ascontiguousarray(np.asarray(tobs, dtype=np.float64).reshape(T))
+    dms = [None] * T if dms is None else list(dms)
+    p = periods.contiguous()
+    s = snrs.contiguous()
+    rp = rows.ctypes.data_as(_lib._u64p)
+    segoff = np.zeros(T + 1, dtype=np.uint64)
+    dp = ctypes.POINTER(ctypes.c_double)
+    _lib.check(lib.rt_peak_segments(libcpp._ptr(p), None, nw, rp, T, tob.ctypes.data_as(dp),
+                                    float(segwidth), float(nstd),
+                                    segoff.ctypes.data_as(_lib._u64p), None, None, st))
+    nseg = int(segoff[-1])
+    fc = torch.empty(nseg, dtype=torch.float64, device=p.device)
+    sc = torch.empty((nseg, nw), dtype=torch.float64, device=p.device)
+    _lib.check(lib.rt_peak_segments(libcpp._ptr(p), libcpp._ptr(s), nw, rp, T,
+                                    tob.ctypes.data_as(dp), float(segwidth), float(nstd),
+                                    segoff.ctypes.data_as(_lib._u64p), libcpp._ptr(fc),
+                                    libcpp._ptr(sc), st))
+    fc_h, sc_h = fc.cpu().numpy(), sc.cpu().numpy()
+    # threshold polynomials (fit_threshold, peak_detection.py:89-109), one fit per width
+    ncoef = polydeg + 1
+    coef = np.zeros((T, nw, ncoef), dtype=np.float64)
+    polycos = [dict() for _ in range(T)]
+    for t in range(T):
+        a, b = int(segoff[t]), int(segoff[t + 1])
+        for iw in range(nw):
+            if b - a >= minseg:
+                c = np.poly1d(np.polyfit(np.log(fc_h[a:b]), sc_h[a:b, iw], polydeg)).coefficients
+            else:
+                c = np.array([smin], dtype=np.float64)
+            polycos[t][iw] = c if b - a >= minseg else [smin]
+            coef[t, iw, ncoef - len(c):] = c
+    dcoef = torch.from_numpy(coef).to(p.device)
+    sel = torch.empty(capacity, dtype=torch.int64, device=p.device)
+    count = ctypes.c_size_t(0)
+    _lib.check(lib.rt_peak_select(libcpp._ptr(p), libcpp._ptr(s), nw, rp, T, libcpp._ptr(dcoef),
+                                  ncoef, float(smin), libcpp._ptr(sel), capacity,
+                                  ctypes.byref(count), st))
+    e = torch.sort(sel[:count.value]).values
+    r = e // nw
+    iws = (e - r * nw).cpu().numpy()
+    rows_sel = r.cpu().numpy()
+    f_sel = (1.0 / p[r]).cpu().numpy()
+    s_sel = s.view(-1)[e].double().cpu().numpy()
+    fb_sel = foldbins[r].cpu().numpy()
+    trial = np.searchsorted(rows[1:].astype(np.int64), rows_sel, side="right")
+    w = np.asarray(widths)
+    out = []
+    for t in range(T):
+        peaks = []
+        mt = trial == t
+        for iw in range(nw):
+            m = mt & (iws == iw)
+            ix_all = rows_sel[m] - int(rows[t])  # ascending row order, as np.where gives
+            fsel, ssel, fbsel = f_sel[m], s_sel[m], fb_sel[m]
+            for cl in _cluster1d(fsel, clrad / tob[t]):
+                k = cl[ssel[cl].argmax()]
+                pf = float(fsel[k])
+                peaks.append(Peak(period=float(1.0 / pf), freq=pf, width=int(w[iw]),
+                                  ducy=float(float(w[iw]) / fbsel[k]), iw=int(iw), ip=int(ix_all[k]),
+                                  snr=float(ssel[k]), dm=dms[t]))
+        out.append((sorted(peaks, key=lambda q: q.snr, reverse=True), polycos[t]))
+    return out
+
+
+def find_peaks(pgram, smin=6.0, segwidth=5.0, nstd=6.0, minseg=10, polydeg=2, clrad=0.1):
+    """Peaks of one Periodogram, as the reference's find_peaks (peak_detection.py:149-240)
+    returns them: (list of Peak sorted by decreasing S/N, {iw: polynomial coefficients})."""
+    torch = libcpp._t()
+    dev = torch.device("cuda")
+
+    def on_dev(a, dtype):
+        if libcpp._is_cuda_tensor(a):
+            return a.to(dtype)
+        return torch.as_tensor(np.ascontiguousarray(a)).to(device=dev, dtype=dtype)
+
+    p = on_dev(pgram.periods, torch.float64)
+    fb = on_dev(np.asarray(pgram.foldbins).astype(np.int64) if not libcpp._is_cuda_tensor(pgram.foldbins)
+                else pgram.foldbins, torch.int64)
+    s = on_dev(pgram.snrs, torch.float32)
+    dm = pgram.metadata.get("dm") if isinstance(pgram.metadata, dict) else None
+    res = find_peaks_batched(p, fb, s, [0, p.numel()], [pgram.tobs], pgram.widths, dms=[dm],
+                             smin=smin, segwidth=segwidth, nstd=nstd, minseg=minseg,
+                             polydeg=polydeg, clrad=clrad)
+    return res[0]
