@@ -308,6 +308,32 @@ def bench_ours(args):
         pipe.close()
         del host_in, host_out
 
+    # ---- peak detection on the step's periodograms (opt-in; outside the timed step) ----
+    peaks_line = None
+    if args.peaks and rank == 0:
+        tobs = np.asarray(lengths, dtype=np.float64) * cfg["tsamp"]
+        rb.find_peaks_batched(outs[0], outs[1], outs[2], bs.row_offsets, tobs, bs.widths)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        res = rb.find_peaks_batched(outs[0], outs[1], outs[2], bs.row_offsets, tobs, bs.widths)
+        torch.cuda.synchronize()
+        gpu_s = time.perf_counter() - t1
+        # the reference's numpy find_peaks on host copies of a few periodograms
+        from oracle import oracle as O
+
+        nref = min(4, ntrials)
+        P = outs[0][:int(bs.row_offsets[nref])].cpu().numpy()
+        F = outs[1][:int(bs.row_offsets[nref])].cpu().numpy().view(np.uint32)
+        S = outs[2][:int(bs.row_offsets[nref])].cpu().numpy()
+        t1 = time.perf_counter()
+        for t in range(nref):
+            a, b = int(bs.row_offsets[t]), int(bs.row_offsets[t + 1])
+            O.find_peaks(P[a:b], F[a:b], S[a:b], bs.widths, float(tobs[t]))
+        cpu_s = (time.perf_counter() - t1) / nref
+        peaks_line = {"trials": ntrials, "gpu_ms_all_trials": gpu_s * 1e3,
+                      "cpu_ms_per_trial_1_core": cpu_s * 1e3,
+                      "peaks_found": int(sum(len(r[0]) for r in res))}
+
     # ---- plain per-(cycle, bins) GPU path on a few trials, for the batching ratio ----
     plain = None
     if rank == 0 and args.plain_trials > 0:
@@ -366,6 +392,7 @@ def bench_ours(args):
             "cpu_baseline": cpu,
             "plain_gpu": plain,
             "batched_vs_plain": (value / world / plain["trials_per_s"]) if plain else None,
+            "find_peaks": peaks_line,
         }
         print(json.dumps(line), flush=True)
     bs.close()
@@ -390,6 +417,7 @@ def main():
     ap.add_argument("--chunk-trials", type=int, default=32)
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--peaks", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()

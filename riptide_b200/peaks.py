@@ -88,9 +88,10 @@ def find_peaks_batched(periods, foldbins, snrs, row_offsets, tobs, widths, dms=N
     polycos = [dict() for _ in range(T)]
     for t in range(T):
         a, b = int(segoff[t]), int(segoff[t + 1])
+        logfc = np.log(fc_h[a:b])
         for iw in range(nw):
             if b - a >= minseg:
-                c = np.poly1d(np.polyfit(np.log(fc_h[a:b]), sc_h[a:b, iw], polydeg)).coefficients
+                c = np.poly1d(np.polyfit(logfc, sc_h[a:b, iw], polydeg)).coefficients
             else:
                 c = np.array([smin], dtype=np.float64)
             polycos[t][iw] = c if b - a >= minseg else [smin]
@@ -110,22 +111,29 @@ def find_peaks_batched(periods, foldbins, snrs, row_offsets, tobs, widths, dms=N
     fb_sel = foldbins[r].cpu().numpy()
     trial = np.searchsorted(rows[1:].astype(np.int64), rows_sel, side="right")
     w = np.asarray(widths)
-    out = []
-    for t in range(T):
-        peaks = []
-        mt = trial == t
-        for iw in range(nw):
-            m = mt & (iws == iw)
-            ix_all = rows_sel[m] - int(rows[t])  # ascending row order, as np.where gives
-            fsel, ssel, fbsel = f_sel[m], s_sel[m], fb_sel[m]
-            for cl in _cluster1d(fsel, clrad / tob[t]):
-                k = cl[ssel[cl].argmax()]
-                pf = float(fsel[k])
-                peaks.append(Peak(period=float(1.0 / pf), freq=pf, width=int(w[iw]),
-                                  ducy=float(float(w[iw]) / fbsel[k]), iw=int(iw), ip=int(ix_all[k]),
-                                  snr=float(ssel[k]), dm=dms[t]))
-        out.append((sorted(peaks, key=lambda q: q.snr, reverse=True), polycos[t]))
-    return out
+    # group the selected points by (trial, width), rows ascending within a group (the order
+    # np.where gives the reference)
+    gkey = trial.astype(np.int64) * nw + iws
+    order = np.lexsort((rows_sel, gkey))
+    gk = gkey[order]
+    bounds = np.flatnonzero(np.diff(gk)) + 1
+    starts = np.concatenate([[0], bounds]) if gk.size else np.zeros(0, np.int64)
+    ends = np.concatenate([bounds, [gk.size]]) if gk.size else np.zeros(0, np.int64)
+    per_trial = [[] for _ in range(T)]
+    for a, b in zip(starts, ends):
+        sl = order[a:b]
+        t, iw = int(gk[a] // nw), int(gk[a] % nw)
+        ix_all = rows_sel[sl] - int(rows[t])
+        fsel, ssel, fbsel = f_sel[sl], s_sel[sl], fb_sel[sl]
+        for cl in _cluster1d(fsel, clrad / tob[t]):
+            k = cl[ssel[cl].argmax()]
+            pf = float(fsel[k])
+            per_trial[t].append(Peak(period=float(1.0 / pf), freq=pf, width=int(w[iw]),
+                                     ducy=float(float(w[iw]) / fbsel[k]), iw=iw,
+                                     ip=int(ix_all[k]), snr=float(ssel[k]), dm=dms[t]))
+    # groups come in width order within a trial, as the reference's loop over widths
+    return [(sorted(per_trial[t], key=lambda q: q.snr, reverse=True), polycos[t])
+            for t in range(T)]
 
 
 def find_peaks(pgram, smin=6.0, segwidth=5.0, nstd=6.0, minseg=10, polydeg=2, clrad=0.1):
