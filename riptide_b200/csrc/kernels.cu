@@ -581,9 +581,82 @@ __global__ void k_running_median(const float* __restrict__ x, const size_t* __re
     }
 }
 
+// Running median through a sorted tile: a CTA sorts the tile + w - 1 (edge-padded) values of
+// its windows once, by (value, position); the median of the window starting at t is the
+// (w / 2 + 1)-th entry of that order whose position lies in [t, t + w). The same order
+// statistic as the counting kernel above, found in ~(w / 2) * (tile + w) / w steps.
+constexpr int kRmedSortTile = 256;
+constexpr int kRmedSortSpan = 512;  // tile + width - 1 <= span
+
+__global__ void __launch_bounds__(kRmedSortTile)
+    k_running_median_sorted(const float* __restrict__ x, const size_t* __restrict__ lengths,
+                            const size_t* __restrict__ offsets, int width,
+                            float* __restrict__ out)
+{
+    __shared__ float sv[kRmedSortSpan];
+    __shared__ short sp[kRmedSortSpan];
+    const int trial = blockIdx.y;
+    const size_t N = lengths[trial];
+    const size_t t0 = (size_t)blockIdx.x * kRmedSortTile;
+    if (t0 >= N) return;
+    const float* xr = x + offsets[trial];
+    const int half = width / 2;
+    const int span = kRmedSortTile + width - 1;
+    for (int i = threadIdx.x; i < kRmedSortSpan; i += blockDim.x) {
+        if (i < span) {
+            long long g = (long long)t0 + i - half;
+            g = g < 0 ? 0 : (g >= (long long)N ? (long long)N - 1 : g);
+            sv[i] = xr[g];
+            sp[i] = (short)i;
+        } else {
+            sv[i] = INFINITY;
+            sp[i] = (short)kRmedSortSpan;
+        }
+    }
+    __syncthreads();
+    // bitonic sort by (value, position)
+    for (int k = 2; k <= kRmedSortSpan; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < kRmedSortSpan; i += blockDim.x) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const bool up = (i & k) == 0;
+                    const float a = sv[i], b = sv[l];
+                    const short pa = sp[i], pb = sp[l];
+                    const bool gt = (a > b) || (a == b && pa > pb);
+                    if (gt == up) {
+                        sv[i] = b;
+                        sv[l] = a;
+                        sp[i] = pb;
+                        sp[l] = pa;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    const int t = threadIdx.x;
+    if (t0 + t >= N) return;
+    int cnt = 0;
+    float med = 0.0f;
+    for (int k = 0; k < span; ++k) {
+        const int q = sp[k];
+        if (q >= t && q < t + width && ++cnt == half + 1) {
+            med = sv[k];
+            break;
+        }
+    }
+    out[offsets[trial] + t0 + t] = med;
+}
+
 int launch_running_median(const float* x, const size_t* d_lengths, const size_t* d_offsets,
                           int ntrials, size_t max_len, int width, float* out, cudaStream_t st)
 {
+    if (width >= 1 && kRmedSortTile + width - 1 <= kRmedSortSpan) {
+        dim3 grid((unsigned)((max_len + kRmedSortTile - 1) / kRmedSortTile), (unsigned)ntrials);
+        k_running_median_sorted<<<grid, kRmedSortTile, 0, st>>>(x, d_lengths, d_offsets, width, out);
+        return check_cuda(cudaGetLastError(), "running_median");
+    }
     int tile = 256;
     size_t smem = (tile + width) * sizeof(float);
     if (smem > kFfaSmemBytes)
