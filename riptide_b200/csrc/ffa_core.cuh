@@ -404,18 +404,21 @@ __device__ __forceinline__ void level_rows_pairs(const RowOp* ops, int nrows,
         float* out = dst + (size_t)r * stride;
         const float* H = src + (size_t)op.h * sstride + lane;
         const float* Tr = src + (size_t)op.t * sstride;
-        // i0 = (shift + 64 j + lane) mod b, stepped by 64 per chunk (one wrap at most: b > 64)
-        int i0 = op.shift + lane;
-        i0 -= (i0 >= b) ? b : 0;
+        // i0 = (shift + 64 j + lane) mod b from one base per row (no chain across chunks;
+        // base + 64 j < 3 b: at most two wraps), unsigned min as the conditional subtract
+        const unsigned ub = (unsigned)b;
+        unsigned base = (unsigned)(op.shift + lane);
+        base = min(base, base - ub);
 #pragma unroll
         for (int j = 0; j < NIT2; ++j) {
             const int c = 64 * j + lane;
-            int i1 = i0 + 32;
-            i1 -= (i1 >= b) ? b : 0;
+            unsigned i0 = base + 64u * j;
+            i0 = min(i0, i0 - ub);
+            if (64 * j >= b - 32) i0 = min(i0, i0 - ub);
+            unsigned i1 = i0 + 32u;
+            i1 = min(i1, i1 - ub);
             if (j < NIT2 - 1 || c < b) out[c] = __fadd_rn(H[64 * j], Tr[i0]);
             if (j < NIT2 - 1 || c + 32 < b) out[c + 32] = __fadd_rn(H[64 * j + 32], Tr[i1]);
-            i0 += 64;
-            i0 -= (i0 >= b) ? b : 0;
         }
     }
 }
