@@ -29,6 +29,7 @@ extern "C" {
 #define RT_ENOMEM 3     /* device or host allocation failed                */
 #define RT_ETIMEOUT 4   /* a bounded wait inside a persistent kernel ran out */
 #define RT_EINTERNAL 5  /* a device-side plan check failed                 */
+#define RT_EIO 6        /* a file could not be opened or read (OSError)    */
 
 /* Message of the last failing call on this thread. */
 const char* rt_last_error(void);
@@ -255,7 +256,7 @@ void rt_search_pipeline_destroy(rt_search_pipeline* pipeline);
  * range is cut into m = ceil(|f[-1] - f[0]| T / segwidth) segments of p = rows // m points;
  * h_seg_offsets (ntrials + 1, output) gives each trial's first segment. With d_fc and d_sc
  * given: d_fc[seg] = median frequency, d_sc[seg * num_widths + iw] = median S/N + nstd *
- * IQR / 1.349 (np.median / np.percentile 'linear'). At most 4096 points per segment. */
+ * IQR / 1.349 (np.median / np.percentile 'linear'). At most 16384 points per segment. */
 int rt_peak_segments(const double* d_periods, const float* d_snrs, size_t num_widths,
                      const uint64_t* h_row_offsets, size_t ntrials, const double* h_tobs,
                      double segwidth, double nstd, uint64_t* h_seg_offsets, double* d_fc,
@@ -303,6 +304,56 @@ int rt_search_backward_rows(rt_search_plan* plan, const float* d_z, const float*
  * d_gy = (g - mean(g) - z * mean(g z)) / std, with d_z the normalised series. */
 int rt_normalise_adjoint(const float* d_g, const float* d_z, size_t size, double std_,
                          float* d_gy, void* stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Time series files into device memory: the data side of TimeSeries.from_presto_inf /
+ * from_sigproc (time_series.py:300-379; reading/presto.py:148-152 reads a .dat as float32;
+ * time_series.py:366-377 reads SIGPROC 8-bit data as int8 / uint8 and casts to float32).
+ * Headers are parsed by the caller (riptide_b200/reading); these calls move the payload.
+ * --------------------------------------------------------------------------------------- */
+#define RT_SAMPLES_F32 0 /* float32 samples                                  */
+#define RT_SAMPLES_U8 1  /* unsigned 8-bit samples (SIGPROC nbits=8, signed=0) */
+#define RT_SAMPLES_I8 2  /* signed 8-bit samples (SIGPROC nbits=8, signed=1)   */
+
+/* Size of a file in bytes. RT_EIO if it cannot be examined. */
+int rt_file_size(const char* path, uint64_t* size);
+/* Read nbytes at `offset` of a file into host memory dst, split over `threads` parallel
+ * pread calls (slices of at least 1 MiB). RT_EIO if the file cannot be opened or holds fewer
+ * bytes. */
+int rt_read_file(const char* path, uint64_t offset, uint64_t nbytes, void* dst, int threads);
+/* Widen n device samples of `encoding` to float32 (astype(np.float32): exact for every 8-bit
+ * value). 8-bit sources must be 4-byte aligned. */
+int rt_samples_to_f32(const void* d_src, int encoding, size_t n, float* d_dst, void* stream);
+/* Load nfiles payloads (nsamples[i] samples of encodings[i] at byte offsets[i] of paths[i])
+ * into d_out, packed back to back as float32 (the layout rt_search_run takes). Each file is
+ * read in chunks into one half of the page-locked host buffer h_staging (staging_bytes
+ * >= 128 KiB) with `threads` parallel reads, while the other half's chunk is copied to
+ * the device; 8-bit chunks are copied as bytes and widened on the device. Returns when the
+ * last chunk has left h_staging; the conversion may still be running on `stream`. */
+int rt_ingest_files(const char* const* paths, const uint64_t* offsets, const uint64_t* nsamples,
+                    const int* encodings, size_t nfiles, float* d_out, void* h_staging,
+                    size_t staging_bytes, int threads, void* stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Folding (TimeSeries.fold, folding.py:21-85): downsample by (period / bins) / tsamp, take
+ * the first m * bins samples as m rows of `bins` phases scaled by (m * factor)^-1/2, then
+ * sum the rows (subints == 1 or m == 1: one profile), keep them (subints < 0, standing for
+ * None, or subints == m), or downsample each phase column by m / subints
+ * (downsample_vertical, folding.py:6-18). RT_EINVAL with the reference's messages for a
+ * period longer than the data, a bin shorter than tsamp, subints == 0, or subints above the
+ * number of periods in the data.
+ * --------------------------------------------------------------------------------------- */
+/* Output rows (1 when ndim == 1) and ndim of fold(size samples, ...), host only. */
+int rt_fold_shape(size_t size, double tsamp, double period, size_t bins, long long subints,
+                  size_t* rows, int* ndim);
+/* fold of d_in (size float32 samples) into d_out (rows x bins, rt_fold_shape). */
+int rt_fold(const float* d_in, size_t size, double tsamp, double period, size_t bins,
+            long long subints, float* d_out, void* stream);
+/* `count` folds of the same series in one launch (candidate folding): fold c at h_periods[c]
+ * with h_bins[c] bins and h_subints[c], written at d_out + h_out_offsets[c]. */
+int rt_fold_batched(const float* d_in, size_t size, double tsamp, const double* h_periods,
+                    const size_t* h_bins, const long long* h_subints, size_t count,
+                    const uint64_t* h_out_offsets, float* d_out, void* stream);
 
 #ifdef __cplusplus
 }

@@ -325,3 +325,42 @@ def find_peaks(periods, foldbins, snrs, widths, tobs, dm=None, smin=6.0, segwidt
         polycos[iw] = polyco
     peaks = sorted(peaks, key=lambda p: p[6], reverse=True)
     return peaks, polycos
+
+
+def downsample_vertical(X, factor):
+    """folding.py:6-18: each column downsampled by `factor` (the C restatement of
+    downsample.hpp)."""
+    m = X.shape[0]
+    if not factor > 1:
+        raise ValueError("factor must be > 1")
+    if not factor < m:
+        raise ValueError("factor must be strictly smaller than the number of input lines")
+    Y = np.ascontiguousarray(X.T)
+    return np.ascontiguousarray(np.asarray([C().downsample(col, factor) for col in Y]).T)
+
+
+def fold(data, tsamp, period, bins, subints=None):
+    """folding.py:21-85 (TimeSeries.fold): downsample by (period / bins) / tsamp, reshape to
+    (m, bins), scale by (m * factor) ** -0.5 in float32, then sum / keep / column-downsample."""
+    length = data.size * tsamp
+    if period > length:
+        raise ValueError("Period exceeds data length")
+    tbin = period / bins
+    if not tbin > tsamp:
+        raise ValueError("Bin width is shorter than sampling time")
+    if subints is not None:
+        subints = int(subints)
+        if not subints >= 1:
+            raise ValueError("subints must be >= 1 or None")
+        if subints > length / period:
+            raise ValueError("subints exceeds the number of signal periods that fit in the data")
+    factor = tbin / tsamp
+    down = C().downsample(np.asarray(data, dtype=np.float32), factor)
+    m = down.size // bins
+    folded = down[:m * bins].reshape(m, bins).copy()
+    folded *= (m * factor) ** -0.5
+    if subints == 1 or m == 1:
+        return folded.sum(axis=0)
+    if subints is None or subints == m:
+        return folded
+    return downsample_vertical(folded, m / subints)

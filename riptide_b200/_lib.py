@@ -13,7 +13,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_riptide_b200.so")
 
-RT_OK, RT_EINVAL, RT_ECUDA, RT_ENOMEM, RT_ETIMEOUT, RT_EINTERNAL = 0, 1, 2, 3, 4, 5
+RT_OK, RT_EINVAL, RT_ECUDA, RT_ENOMEM, RT_ETIMEOUT, RT_EINTERNAL, RT_EIO = 0, 1, 2, 3, 4, 5, 6
+RT_SAMPLES_F32, RT_SAMPLES_U8, RT_SAMPLES_I8 = 0, 1, 2
 
 _sz = ctypes.c_size_t
 _vp = ctypes.c_void_p
@@ -62,6 +63,13 @@ SIGNATURES = {
     "rt_downsample_adjoint": (ctypes.c_int, [_vp, _sz, _d, _vp, _vp]),
     "rt_normalise_adjoint": (ctypes.c_int, [_vp, _vp, _sz, _d, _vp, _vp]),
     "rt_search_set_graph": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "rt_fold_shape": (ctypes.c_int, [_sz, _d, _d, _sz, ctypes.c_longlong, ctypes.POINTER(_sz), ctypes.POINTER(ctypes.c_int)]),
+    "rt_fold": (ctypes.c_int, [_vp, _sz, _d, _d, _sz, ctypes.c_longlong, _vp, _vp]),
+    "rt_fold_batched": (ctypes.c_int, [_vp, _sz, _d, _vp, _vp, _vp, _sz, _u64p, _vp, _vp]),
+    "rt_file_size": (ctypes.c_int, [ctypes.c_char_p, _u64p]),
+    "rt_read_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_uint64, _vp, ctypes.c_int]),
+    "rt_samples_to_f32": (ctypes.c_int, [_vp, ctypes.c_int, _sz, _vp, _vp]),
+    "rt_ingest_files": (ctypes.c_int, [ctypes.POINTER(ctypes.c_char_p), _u64p, _u64p, ctypes.POINTER(ctypes.c_int), _sz, _vp, _vp, _sz, ctypes.c_int, _vp]),
     "rt_search_graph_captures": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
     "rt_search_pipeline_create": (ctypes.c_int, [_u64p, _sz, _vp, _u64p, _sz, _sz, ctypes.POINTER(_vp)]),
     "rt_search_pipeline_rows": (ctypes.c_int, [_vp, _u64p]),
@@ -143,6 +151,8 @@ def check(status):
         raise ValueError(msg)
     if status == RT_ENOMEM:
         raise MemoryError(msg)
+    if status == RT_EIO:
+        raise OSError(msg)
     raise RiptideError(f"[status {status}] {msg}")
 
 

@@ -12,8 +12,8 @@
 
 namespace rt {
 
-constexpr int kSegThreads = 256;
-constexpr int kSegMaxPoints = 4096;  // points per segment sorted in shared memory
+constexpr int kSegThreads = 512;
+constexpr int kSegMaxPoints = 16384;  // points per segment sorted in shared memory (128 KB)
 
 // In-place ascending bitonic sort of n (power of two) doubles in shared memory.
 __device__ void bitonic_sort(double* a, int n)
@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(kSegThreads)
                     const SegTrial* __restrict__ trials, int ntrials, double nstd,
                     double* __restrict__ fc, double* __restrict__ sc)
 {
-    __shared__ double v[kSegMaxPoints];
+    extern __shared__ double v[];  // the segment padded to a power of two
     const int seg = blockIdx.x, iw = blockIdx.y;
     int lo = 0, hi = ntrials - 1;  // trial of this segment
     while (lo < hi) {
@@ -157,7 +157,7 @@ extern "C" int rt_peak_segments(const double* d_periods, const float* d_snrs, si
     }
     RT_TRY_CUDA(cudaStreamSynchronize(st));
     std::vector<SegTrial> tr(ntrials);
-    uint64_t seg = 0;
+    uint64_t seg = 0, pmax = 1;
     h_seg_offsets[0] = 0;
     for (size_t t = 0; t < ntrials; ++t) {
         const double w = segwidth / h_tobs[t];
@@ -172,6 +172,7 @@ extern "C" int rt_peak_segments(const double* d_periods, const float* d_snrs, si
         if (p > (uint64_t)kSegMaxPoints)
             return set_error(RT_EINVAL, "segments of %llu points exceed the device limit (%d)",
                              (unsigned long long)p, kSegMaxPoints);
+        pmax = std::max(pmax, p);
         tr[t].row0 = h_row_offsets[t];
         tr[t].seg0 = (int)seg;
         tr[t].m = (int)m;
@@ -187,10 +188,18 @@ extern "C" int rt_peak_segments(const double* d_periods, const float* d_snrs, si
     RT_TRY_CUDA(cudaMallocAsync((void**)&d_tr, ntrials * sizeof(SegTrial), st));
     int s = check_cuda(cudaMemcpyAsync(d_tr, tr.data(), ntrials * sizeof(SegTrial),
                                        cudaMemcpyHostToDevice, st), "peak_segments");
+    size_t n2 = 1;
+    while (n2 < pmax) n2 <<= 1;
+    const size_t smem = n2 * sizeof(double);
+    if (s == RT_OK && smem > 48 * 1024)
+        s = check_cuda(cudaFuncSetAttribute(k_peak_segments,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)(kSegMaxPoints * sizeof(double))),
+                       "peak_segments");
     if (s == RT_OK && seg > 0) {
         dim3 grid((unsigned)seg, (unsigned)num_widths);
-        k_peak_segments<<<grid, kSegThreads, 0, st>>>(d_periods, d_snrs, (int)num_widths, d_tr,
-                                                      (int)ntrials, nstd, d_fc, d_sc);
+        k_peak_segments<<<grid, kSegThreads, smem, st>>>(d_periods, d_snrs, (int)num_widths,
+                                                         d_tr, (int)ntrials, nstd, d_fc, d_sc);
         s = check_cuda(cudaGetLastError(), "peak_segments");
     }
     cudaFreeAsync(d_tr, st);

@@ -1,5 +1,5 @@
 """TimeSeries (time_series.py of the reference): float32 data on the host, operations on
-the GPU through the C ABI. Reading PRESTO / SIGPROC files and folding are not included."""
+the GPU through the C ABI; PRESTO and SIGPROC files read by the library's parallel reader."""
 import copy
 
 import numpy as np
@@ -86,6 +86,33 @@ class TimeSeries(object):
     @classmethod
     def from_npy_file(cls, fname, tsamp):
         return cls(np.load(fname), tsamp, copy=False)
+
+    @classmethod
+    @timing
+    def from_presto_inf(cls, fname):
+        """TimeSeries of a PRESTO .inf file and its .dat samples (time_series.py:300-336).
+        Warns for X-ray and gamma-ray data."""
+        from .reading import SeriesFile, read_payload
+        sf = SeriesFile.from_presto_inf(fname)
+        return cls(read_payload(sf.path, sf.offset, sf.nsamp, sf.encoding), tsamp=sf.tsamp,
+                   metadata=sf.metadata)
+
+    @classmethod
+    @timing
+    def from_sigproc(cls, fname, extra_keys=None):
+        """TimeSeries of a SIGPROC dedispersed time series, 32-bit float or 8-bit with a
+        'signed' header key (time_series.py:338-379). `extra_keys`: {key: type} of
+        non-standard header keys."""
+        from .reading import SeriesFile, read_payload
+        sf = SeriesFile.from_sigproc(fname, extra_keys=extra_keys)
+        return cls(read_payload(sf.path, sf.offset, sf.nsamp, sf.encoding), tsamp=sf.tsamp,
+                   metadata=sf.metadata)
+
+    def fold(self, period, bins, subints=None):
+        """Fold at `period` seconds into `bins` phase bins (time_series.py:153-174,
+        folding.py:21-85)."""
+        from .folding import fold
+        return fold(self, period, bins, subints=subints)
 
     @property
     def nsamp(self):

@@ -52,7 +52,8 @@ def _install_stubs():
     mpl.pyplot = mod("matplotlib.pyplot")
     ap = mod("astropy")
     ap.units = mod("astropy.units")
-    ap.coordinates = mod("astropy.coordinates", SkyCoord=type("SkyCoord", (), {}))
+    ap.coordinates = mod("astropy.coordinates",
+                         SkyCoord=type("SkyCoord", (), {"__init__": lambda self, *a, **k: None}))
     mod("schema", Schema=_Anything, And=_Anything, Or=_Anything, Optional=_Anything)
 
 
@@ -73,14 +74,24 @@ def import_reference():
 
     mods = {}
     for name in ("timing", "ffautils", "libffa", "running_medians", "time_series", "search",
-                 "clustering", "peak_detection"):
+                 "clustering", "peak_detection", "folding", "reading.presto", "reading.sigproc",
+                 "metadata"):
         mods[name] = importlib.import_module("riptide." + name)
     mods["periodogram"] = importlib.import_module("riptide.periodogram")
     return libcpp, mods
 
 
-def main():
+def main(sections=None):
+    """Write the fixtures of `sections` (all when None): core, fold, readers."""
     libcpp, M = import_reference()
+    if sections is None or "fold" in sections:
+        make_fold(M)
+    if sections is None or "readers" in sections:
+        make_readers(M)
+    if sections is None or "workerpool" in sections:
+        make_workerpool(M)
+    if sections is not None and "core" not in sections:
+        return
     rng = np.random.default_rng(20240531)
     out = {}
 
@@ -230,5 +241,166 @@ def main():
             print(f, os.path.getsize(os.path.join(HERE, f)))
 
 
+def make_fold(M):
+    """TimeSeries.fold of the reference (folding.py:21-85) on a seeded series, for each case
+    (period, bins, subints) of FOLD_CASES."""
+    rng = np.random.default_rng(777)
+    TS = M["time_series"].TimeSeries
+    out = {}
+    for s, (nsamp, tsamp) in enumerate(FOLD_SERIES):
+        x = (rng.standard_normal(nsamp) + 0.5).astype(np.float32)
+        out[f"x{s}"] = x
+        out[f"tsamp{s}"] = np.float64(tsamp)
+    for i, (s, period, bins, subints) in enumerate(FOLD_CASES):
+        ts = TS(out[f"x{s}"], float(out[f"tsamp{s}"]))
+        out[f"y{i}"] = np.asarray(ts.fold(period, bins, subints=subints), dtype=np.float32)
+    np.savez_compressed(os.path.join(HERE, "fold.npz"), **out, n=len(FOLD_CASES))
+
+
+# (series index, period s, bins, subints or None)
+FOLD_SERIES = [(20000, 1e-3), (1 << 16, 64e-6)]
+FOLD_CASES = [
+    (0, 1.0, 100, None), (0, 1.0, 100, 2), (0, 1.0, 100, 20), (0, 1.0, 100, 1),
+    (0, 1.0, 100, 3), (0, 1.0, 100, 7), (0, 0.37, 64, None), (0, 0.37, 64, 13),
+    (0, 2.5, 250, 4), (0, 19.9, 128, None), (0, 0.101, 100, None), (0, 7.0, 60, 2),
+    (1, 0.0731, 128, None), (1, 0.0731, 128, 16), (1, 1.9, 256, 1), (1, 0.5, 512, 3),
+]
+
+
+def make_readers(M):
+    """Files written by riptide_b200.reading.writers, read back by the reference's own readers
+    (reading/presto.py, reading/sigproc.py, TimeSeries.from_presto_inf / from_sigproc). The
+    file bytes are stored so that the tests pin the writer too."""
+    import json
+    import tempfile
+    import warnings
+
+    from riptide_b200.reading.writers import write_presto, write_sigproc
+
+    TS = M["time_series"].TimeSeries
+    out = {}
+    docs = []
+    rng = np.random.default_rng(31337)
+    with tempfile.TemporaryDirectory() as d:
+        for i, (kind, items, data) in enumerate(_reader_cases(rng)):
+            if kind == "presto":
+                base = os.path.join(d, f"case{i}")
+                write_presto(base, data, items)
+                with warnings.catch_warnings():
+                    warnings.simplefilter("ignore")
+                    ts = TS.from_presto_inf(base + ".inf")
+                inf = M["reading.presto"].PrestoInf(base + ".inf")
+                hdr = {k: v for k, v in inf.items()}
+                with open(base + ".inf", "rb") as f:
+                    out[f"inf{i}"] = np.frombuffer(f.read(), dtype=np.uint8)
+                with open(base + ".dat", "rb") as f:
+                    out[f"dat{i}"] = np.frombuffer(f.read(), dtype=np.uint8)
+            else:
+                fn = os.path.join(d, f"case{i}.tim")
+                write_sigproc(fn, data, items)
+                ts = TS.from_sigproc(fn)
+                sh = M["reading.sigproc"].SigprocHeader(fn)
+                hdr = dict(sh)
+                hdr["_bytesize"] = sh.bytesize
+                with open(fn, "rb") as f:
+                    out[f"tim{i}"] = np.frombuffer(f.read(), dtype=np.uint8)
+            out[f"data{i}"] = ts.data
+            out[f"in{i}"] = np.asarray(data)
+            docs.append({"kind": kind, "items": items, "header": hdr, "tsamp": ts.tsamp,
+                         "dm": ts.metadata.get("dm"), "tobs": ts.metadata.get("tobs")})
+    out["json"] = np.frombuffer(json.dumps(docs).encode(), dtype=np.uint8)
+    np.savez_compressed(os.path.join(HERE, "readers.npz"), **out, n=len(docs))
+
+
+# The reference's pipeline test data (tests/test_pipeline.py:36-66): three DM trials of a
+# 1 s pulsar, 128 s at 256 us, each generated after np.random.seed(0).
+WP_TRIALS = [(0.0, 10.0, 0.05), (10.0, 20.0, 0.02), (20.0, 10.0, 0.05)]  # dm, amplitude, ducy
+WP_TOBS, WP_TSAMP, WP_PERIOD = 128.0, 256e-6, 1.0
+WP_DEREDDEN = {"rmed_width": 5.0, "rmed_minpts": 101}
+WP_RANGES = [
+    {"name": "medium", "ffa_search": {"period_min": 0.5, "period_max": 4.0, "bins_min": 480,
+                                      "bins_max": 520, "fpmin": 8, "wtsp": 1.5},
+     "find_peaks": {"smin": 7.0}},
+    {"name": "long", "ffa_search": {"period_min": 4.0, "period_max": 120.0, "bins_min": 960,
+                                    "bins_max": 1040, "fpmin": 8, "wtsp": 1.5},
+     "find_peaks": {"smin": 7.0}},
+]
+
+
+def make_workerpool(M):
+    """Peaks of the reference's WorkerPool.process_fname_list (pipeline/worker_pool.py) over
+    PRESTO files of the reference's pipeline test signal, with the ranges of its test
+    configuration A (tests/pipeline_config_A.yml)."""
+    import importlib.util
+    import tempfile
+
+    from riptide_b200.reading.writers import write_presto
+
+    pkg = sys.modules["riptide"]
+    pkg.TimeSeries = M["time_series"].TimeSeries
+    pkg.Metadata = M["metadata"].Metadata
+    pkg.ffa_search = M["search"].ffa_search
+    pkg.find_peaks = M["peak_detection"].find_peaks
+    # the module file alone: the pipeline package's __init__ imports the whole application
+    spec = importlib.util.spec_from_file_location(
+        "ref_worker_pool", os.path.join(REF_ROOT, "src", "riptide", "pipeline", "worker_pool.py"))
+    WP = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(WP)
+    TS = M["time_series"].TimeSeries
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        fnames = []
+        for i, (dm, amp, ducy) in enumerate(WP_TRIALS):
+            np.random.seed(0)
+            ts = TS.generate(WP_TOBS, WP_TSAMP, WP_PERIOD, amplitude=amp, ducy=ducy, stdnoise=1.0)
+            out[f"sum{i}"] = np.float64(ts.data.astype(np.float64).sum())
+            base = os.path.join(d, f"fake_DM{dm:.3f}")
+            write_presto(base, ts.data, workerpool_inf(os.path.basename(base), ts.nsamp, dm))
+            fnames.append(base + ".inf")
+        pool = WP.WorkerPool(WP_DEREDDEN, WP_RANGES, processes=1, fmt="presto")
+        # process_fname_list without its process pool: the same calls, flattened the same way
+        peaks = [p for f in fnames for p in pool.process_fname(f)]
+    for key in ("period", "freq", "width", "ducy", "iw", "ip", "snr", "dm"):
+        out[key] = np.array([getattr(p, key) for p in peaks])
+    np.savez_compressed(os.path.join(HERE, "workerpool.npz"), **out)
+
+
+def workerpool_inf(basename, nsamp, dm):
+    """.inf items of the pipeline test files (tests/presto_generation.py:7-28)."""
+    return dict(basename=basename, telescope="Parkes", instrument="Multibeam",
+                source_name="Pulsar", raj="00:00:01.0000", decj="-00:00:01.0000",
+                observer="Kenji Oba", mjd=59000.0, barycentered=True, nsamp=int(nsamp),
+                tsamp=WP_TSAMP, breaks=False, onoff_pairs=[], em_band="Radio", fov_arcsec=981.0,
+                dm=float(dm), fbot=1182.1953125, bandwidth=400.0, nchan=1024, cbw=0.390625,
+                analyst="Space Sheriff Gavan")
+
+
+def _reader_cases(rng):
+    radio = dict(basename="case", telescope="Parkes", instrument="Multibeam",
+                 source_name="J0000+0000", raj="00:00:01.0000", decj="-00:00:01.0000",
+                 observer="Nobody", mjd=59000.5, barycentered=True, nsamp=1000, tsamp=6.4e-05,
+                 breaks=False, onoff_pairs=[], em_band="Radio", fov_arcsec=981.0, dm=42.42,
+                 fbot=1182.1953125, bandwidth=400.0, nchan=1024, cbw=0.390625, analyst="Nobody")
+    breaks = dict(radio, breaks=True, onoff_pairs=[(0, 700), (800, 999)], nsamp=1000, dm=0.0)
+    xray = {k: v for k, v in radio.items()
+            if k not in ("fov_arcsec", "dm", "fbot", "bandwidth", "nchan", "cbw", "analyst")}
+    xray.update(em_band="X-ray", fov_arcsec=3.0, central_energy_kev=1.0,
+                energy_bandpass_kev=5.0, analyst="Nobody")
+    sig = dict(source_name="Fake", telescope_id=4, machine_id=10, src_raj=63642.23,
+               src_dej=-454405.0, az_start=0.0, za_start=0.0, data_type=2, refdm=26.31,
+               fch1=1581.8046875, barycentric=0, nchans=1, nbits=32, tstart=56771.1303125,
+               tsamp=6.4e-05, nifs=1)
+    u8 = dict(sig, nbits=8, signed=False, refdm=187.5)
+    i8 = dict(sig, nbits=8, signed=True, refdm=3.0)
+    return [
+        ("presto", radio, rng.standard_normal(1000).astype(np.float32)),
+        ("presto", breaks, rng.standard_normal(1000).astype(np.float32)),
+        ("presto", xray, rng.poisson(3.0, 1000).astype(np.float32)),
+        ("sigproc", sig, rng.standard_normal(777).astype(np.float32)),
+        ("sigproc", u8, rng.integers(0, 256, 1001).astype(np.uint8)),
+        ("sigproc", i8, rng.integers(-128, 128, 1003).astype(np.int8)),
+    ]
+
+
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or None)
