@@ -40,6 +40,22 @@ def _cpu_worker(args):
     return time.perf_counter() - t0
 
 
+def _cpu_file_worker(args):
+    """The reference's WorkerPool.process_fname for one PRESTO file and one range
+    (worker_pool.py:47-68): read, deredden, normalise, search, find_peaks."""
+    inf_path, tsamp, kw, fpkw = args
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    sys.path.insert(0, HERE)
+    from oracle import oracle as O
+
+    ref = O.ref_libcpp()
+    t0 = time.perf_counter()
+    data = np.fromfile(inf_path[:-4] + ".dat", dtype=np.float32)
+    z, widths, periods, foldbins, snrs = O.ffa_search(data, tsamp, libcpp=ref, **kw)
+    O.find_peaks(periods, foldbins, snrs, widths, data.size * tsamp, **fpkw)
+    return time.perf_counter() - t0
+
+
 def cpu_kind():
     from oracle import oracle as O
 
@@ -334,6 +350,11 @@ def bench_ours(args):
                       "cpu_ms_per_trial_1_core": cpu_s * 1e3,
                       "peaks_found": int(sum(len(r[0]) for r in res))}
 
+    # ---- the pipeline's search stage from files (opt-in): WorkerPool vs the reference ----
+    wp_line = None
+    if args.workerpool > 0 and rank == 0:
+        wp_line = bench_workerpool(args, cfg, data, lengths, pool if do_cpu else None)
+
     # ---- plain per-(cycle, bins) GPU path on a few trials, for the batching ratio ----
     plain = None
     if rank == 0 and args.plain_trials > 0:
@@ -393,6 +414,7 @@ def bench_ours(args):
             "plain_gpu": plain,
             "batched_vs_plain": (value / world / plain["trials_per_s"]) if plain else None,
             "find_peaks": peaks_line,
+            "workerpool": wp_line,
         }
         print(json.dumps(line), flush=True)
     bs.close()
@@ -401,6 +423,69 @@ def bench_ours(args):
 
         dist.destroy_process_group()
     return 0
+
+
+def bench_workerpool(args, cfg, data, lengths, pool):
+    """Time WorkerPool.process_fname_list on `args.workerpool` PRESTO files of the workload
+    (written to a temporary folder first, so they are read from the page cache) with one
+    search range of the workload's parameters and find_peaks' defaults; and the reference's
+    process_fname on a sample of the files on all host cores."""
+    import shutil
+    import tempfile
+
+    import torch
+
+    import riptide_b200 as rb
+    from riptide_b200.reading.writers import write_presto
+
+    n = min(int(args.workerpool), len(lengths))
+    offs = np.concatenate([[0], np.cumsum(lengths)])
+    kw = {k: v for k, v in cfg["search"].items() if k not in ("rmed_width", "rmed_minpts")}
+    rng_conf = [{"ffa_search": kw, "find_peaks": {}}]
+    dered = {"rmed_width": cfg["search"]["rmed_width"],
+             "rmed_minpts": cfg["search"]["rmed_minpts"]}
+    tmp = tempfile.mkdtemp(prefix="rt_wp_")
+    try:
+        fnames = []
+        for i in range(n):
+            base = os.path.join(tmp, f"trial{i:04d}")
+            x = data[int(offs[i]):int(offs[i + 1])].cpu().numpy()
+            write_presto(base, x, dict(
+                basename=os.path.basename(base), telescope="Synthetic", instrument="none",
+                source_name="synthetic", raj="00:00:00.0000", decj="00:00:00.0000",
+                observer="none", mjd=60000.0, barycentered=False, nsamp=int(x.size),
+                tsamp=cfg["tsamp"], breaks=False, em_band="Radio", fov_arcsec=1.0,
+                dm=float(i), fbot=1200.0, bandwidth=400.0, nchan=1024, cbw=0.390625,
+                analyst="none"))
+            fnames.append(base + ".inf")
+        wp = rb.WorkerPool(dered, rng_conf, fmt="presto", chunk_trials=args.chunk_trials)
+        peaks = wp.process_fname_list(fnames)  # warm-up: plans, first touch
+        torch.cuda.synchronize()
+        times = []
+        for _ in range(2):
+            t0 = time.perf_counter()
+            peaks = wp.process_fname_list(fnames)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+        wp.close()
+        gpu_s = min(times)
+        line = {"files": n, "files_per_s": n / gpu_s, "s_per_call": gpu_s,
+                "peaks_found": len(peaks),
+                "api": "WorkerPool.process_fname_list (PRESTO .inf/.dat from the page cache, "
+                       "one range, find_peaks defaults)"}
+        if pool is not None:
+            ncores = os.cpu_count() or 1
+            sample = fnames[:max(1, min(ncores, n))]
+            job = [(f, cfg["tsamp"], dict(cfg["search"]), {}) for f in sample]
+            t0 = time.perf_counter()
+            list(pool.map(_cpu_file_worker, job))
+            cpu_s = time.perf_counter() - t0
+            line["cpu_reference"] = {"files_per_s": len(sample) / cpu_s, "cores": ncores,
+                                     "kind": cpu_kind(), "sample": f"{len(sample)} files, "
+                                     "one per process (process_fname of the reference)"}
+        return line
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
 
 
 def main():
@@ -418,6 +503,8 @@ def main():
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--peaks", action="store_true")
+    ap.add_argument("--workerpool", type=int, default=0,
+                    help="also time WorkerPool.process_fname_list on this many files")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()

@@ -12,23 +12,24 @@
 
 namespace rt {
 
-constexpr int kSegThreads = 512;
-constexpr int kSegMaxPoints = 16384;  // points per segment sorted in shared memory (128 KB)
+constexpr int kSegMaxPoints = 16384;  // points per segment, sorted on chip
 
-// In-place ascending bitonic sort of n (power of two) doubles in shared memory.
-__device__ void bitonic_sort(double* a, int n)
+// In-place ascending bitonic sort of n (a power of two) values in shared memory. Each
+// compare-exchange stage is n/2 independent pairs (i, i + j), i with bit j clear, dealt to
+// the threads so that none idles; padding values are +inf.
+template <typename T>
+__device__ void bitonic_sort(T* a, int n)
 {
+    const int half = n >> 1;
     for (int k = 2; k <= n; k <<= 1) {
         for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = threadIdx.x; i < n; i += blockDim.x) {
-                const int l = i ^ j;
-                if (l > i) {
-                    const bool up = (i & k) == 0;
-                    const double x = a[i], y = a[l];
-                    if ((x > y) == up) {
-                        a[i] = y;
-                        a[l] = x;
-                    }
+            for (int q = threadIdx.x; q < half; q += blockDim.x) {
+                const int i = ((q & ~(j - 1)) << 1) | (q & (j - 1));  // a 0 at bit j
+                const bool up = (i & k) == 0;
+                const T x = a[i], y = a[i + j];
+                if ((x > y) == up) {
+                    a[i] = y;
+                    a[i + j] = x;
                 }
             }
             __syncthreads();
@@ -36,22 +37,15 @@ __device__ void bitonic_sort(double* a, int n)
     }
 }
 
-// numpy's linear interpolation between two order statistics (numpy _lerp)
-__device__ __forceinline__ double np_lerp(double a, double b, double t)
+// numpy's linear interpolation between two order statistics (numpy _lerp): the difference
+// b - a is taken in the input's type, float32 for S/N values (exact operands: the sorted
+// values are float32 values held in doubles), the rest in float64.
+__device__ __forceinline__ double np_lerp_f32(double a, double b, double t)
 {
-    const double d = __dsub_rn(b, a);
+    const double d = (double)__fsub_rn((float)b, (float)a);
     return (t >= 0.5) ? __dsub_rn(b, __dmul_rn(d, __dsub_rn(1.0, t))) : __dadd_rn(a, __dmul_rn(d, t));
 }
 
-// np.percentile(x, q) of n sorted values, method 'linear'
-__device__ __forceinline__ double np_percentile_sorted(const double* a, int n, double q)
-{
-    const double v = __dmul_rn((double)(n - 1), q);
-    const double prev = floor(v);
-    const int i0 = (int)prev;
-    const int i1 = min(i0 + 1, n - 1);
-    return np_lerp(a[i0], a[i1], __dsub_rn(v, prev));
-}
 
 struct SegTrial {
     unsigned long long row0;  // first periodogram row of the trial
@@ -59,14 +53,30 @@ struct SegTrial {
 };
 
 // One CTA per (segment, width): sc = median + nstd * IQR / 1.349 of the segment's S/N
-// (segment_stats, peak_detection.py:38-86). CTAs of width 0 also write the segment's median
-// frequency fc.
-__global__ void __launch_bounds__(kSegThreads)
+// (segment_stats, peak_detection.py:38-86), the S/N sorted as float32 (their type). CTAs of
+// width 0 also write the segment's median frequency fc (sorted as float64). `n2`: the sort
+// size of the launch, a power of two >= every segment's length.
+template <typename T>
+__device__ __forceinline__ double np_percentile_sorted(const T* a, int n, double q);
+
+// np.percentile(x, q) of n sorted float32 values, method 'linear'
+template <>
+__device__ __forceinline__ double np_percentile_sorted<float>(const float* a, int n, double q)
+{
+    const double v = __dmul_rn((double)(n - 1), q);
+    const double prev = floor(v);
+    const int i0 = (int)prev;
+    const int i1 = min(i0 + 1, n - 1);
+    return np_lerp_f32(a[i0], a[i1], __dsub_rn(v, prev));
+}
+
+__global__ void __launch_bounds__(1024)
     k_peak_segments(const double* __restrict__ periods, const float* __restrict__ snrs, int nw,
-                    const SegTrial* __restrict__ trials, int ntrials, double nstd,
+                    const SegTrial* __restrict__ trials, int ntrials, double nstd, int n2,
                     double* __restrict__ fc, double* __restrict__ sc)
 {
-    extern __shared__ double v[];  // the segment padded to a power of two
+    extern __shared__ double sv[];
+    float* vf = reinterpret_cast<float*>(sv);
     const int seg = blockIdx.x, iw = blockIdx.y;
     int lo = 0, hi = ntrials - 1;  // trial of this segment
     while (lo < hi) {
@@ -76,28 +86,26 @@ __global__ void __launch_bounds__(kSegThreads)
     }
     const SegTrial T = trials[lo];
     const int j = seg - T.seg0, p = T.p;
-    int n2 = 1;
-    while (n2 < p) n2 <<= 1;
     const size_t r0 = T.row0 + (size_t)j * p;
     for (int i = threadIdx.x; i < n2; i += blockDim.x)
-        v[i] = (i < p) ? (double)snrs[(r0 + i) * nw + iw] : INFINITY;
+        vf[i] = (i < p) ? snrs[(r0 + i) * nw + iw] : INFINITY;
     __syncthreads();
-    bitonic_sort(v, n2);
+    bitonic_sort(vf, n2);
     if (threadIdx.x == 0) {
-        const double s25 = np_percentile_sorted(v, p, 0.25);
-        const double s50 = np_percentile_sorted(v, p, 0.5);
-        const double s75 = np_percentile_sorted(v, p, 0.75);
+        const double s25 = np_percentile_sorted(vf, p, 0.25);
+        const double s50 = np_percentile_sorted(vf, p, 0.5);
+        const double s75 = np_percentile_sorted(vf, p, 0.75);
         const double sstd = __ddiv_rn(__dsub_rn(s75, s25), 1.349);
         sc[(size_t)seg * nw + iw] = __dadd_rn(s50, __dmul_rn(nstd, sstd));
     }
     if (iw != 0) return;
     __syncthreads();
     for (int i = threadIdx.x; i < n2; i += blockDim.x)
-        v[i] = (i < p) ? __ddiv_rn(1.0, periods[r0 + i]) : INFINITY;
+        sv[i] = (i < p) ? __ddiv_rn(1.0, periods[r0 + i]) : INFINITY;
     __syncthreads();
-    bitonic_sort(v, n2);
+    bitonic_sort(sv, n2);
     if (threadIdx.x == 0)  // np.median: the middle value, or the mean of the middle two
-        fc[seg] = (p & 1) ? v[p / 2] : __ddiv_rn(__dadd_rn(v[p / 2 - 1], v[p / 2]), 2.0);
+        fc[seg] = (p & 1) ? sv[p / 2] : __ddiv_rn(__dadd_rn(sv[p / 2 - 1], sv[p / 2]), 2.0);
 }
 
 // Points above the dynamic threshold poly(log f) and above smin (find_peaks_single,
@@ -188,9 +196,10 @@ extern "C" int rt_peak_segments(const double* d_periods, const float* d_snrs, si
     RT_TRY_CUDA(cudaMallocAsync((void**)&d_tr, ntrials * sizeof(SegTrial), st));
     int s = check_cuda(cudaMemcpyAsync(d_tr, tr.data(), ntrials * sizeof(SegTrial),
                                        cudaMemcpyHostToDevice, st), "peak_segments");
-    size_t n2 = 1;
-    while (n2 < pmax) n2 <<= 1;
-    const size_t smem = n2 * sizeof(double);
+    int n2 = 2;
+    while ((uint64_t)n2 < pmax) n2 <<= 1;
+    const int threads = std::max(32, std::min(1024, n2 / 2));
+    const size_t smem = (size_t)n2 * sizeof(double);
     if (s == RT_OK && smem > 48 * 1024)
         s = check_cuda(cudaFuncSetAttribute(k_peak_segments,
                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -198,8 +207,8 @@ extern "C" int rt_peak_segments(const double* d_periods, const float* d_snrs, si
                        "peak_segments");
     if (s == RT_OK && seg > 0) {
         dim3 grid((unsigned)seg, (unsigned)num_widths);
-        k_peak_segments<<<grid, kSegThreads, smem, st>>>(d_periods, d_snrs, (int)num_widths,
-                                                         d_tr, (int)ntrials, nstd, d_fc, d_sc);
+        k_peak_segments<<<grid, threads, smem, st>>>(d_periods, d_snrs, (int)num_widths, d_tr,
+                                                     (int)ntrials, nstd, n2, d_fc, d_sc);
         s = check_cuda(cudaGetLastError(), "peak_segments");
     }
     cudaFreeAsync(d_tr, st);

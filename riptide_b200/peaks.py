@@ -15,11 +15,59 @@ selected points run on the host with the reference's numpy calls, so that the pe
 ones the reference finds.
 """
 import ctypes
+import os
 import typing
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
 from . import _lib, libcpp
+
+try:  # the LAPACK least-squares gufunc behind np.linalg.lstsq (numpy >= 1.x and 2.x)
+    from numpy.linalg import _umath_linalg as _ulinalg
+except ImportError:  # pragma: no cover
+    _ulinalg = None
+
+_POOL = None
+
+
+def _pool():
+    global _POOL
+    if _POOL is None:
+        _POOL = ThreadPoolExecutor(max(1, min(8, os.cpu_count() or 1)))
+    return _POOL
+
+
+def _polyfit_stacked(X, Y, deg):
+    """np.polyfit(X[k], Y[k], deg) for every row k of X, Y (K x M), in one stacked call of the
+    LAPACK least-squares routine np.polyfit uses: the same Vandermonde matrix, column scaling,
+    rcond and driver call per problem, so every coefficient is the one np.polyfit returns.
+    Large stacks are split over threads (the gufunc runs without the GIL)."""
+    K, M = X.shape
+    order = int(deg) + 1
+    if _ulinalg is None:
+        return np.array([np.polyfit(X[k], Y[k], deg) for k in range(K)]).reshape(K, order)
+    lhs = np.empty((K, M, order))
+    tmp = lhs[:, :, ::-1]  # np.vander: powers by repeated multiplication
+    tmp[:, :, 0] = 1
+    if order > 1:
+        tmp[:, :, 1:] = (X + 0.0)[:, :, None]
+        np.multiply.accumulate(tmp[:, :, 1:], out=tmp[:, :, 1:], axis=2)
+    scale = np.sqrt((lhs * lhs).sum(axis=1))
+    lhs /= scale[:, None, :]
+    rhs = (Y + 0.0)[:, :, None]
+    rcond = M * np.finfo(np.float64).eps
+
+    def solve(sl):
+        with np.errstate(invalid="ignore", over="ignore", divide="ignore", under="ignore"):
+            return _ulinalg.lstsq(lhs[sl], rhs[sl], rcond, signature="ddd->ddid")[0]
+
+    if K >= 512:
+        parts = [slice(a, min(K, a + 256)) for a in range(0, K, 256)]
+        c = np.concatenate(list(_pool().map(solve, parts)))
+    else:
+        c = solve(slice(0, K))
+    return c[:, :, 0] / scale
 
 
 class Peak(typing.NamedTuple):
@@ -82,20 +130,30 @@ def find_peaks_batched(periods, foldbins, snrs, row_offsets, tobs, widths, dms=N
                                     segoff.ctypes.data_as(_lib._u64p), libcpp._ptr(fc),
                                     libcpp._ptr(sc), st))
     fc_h, sc_h = fc.cpu().numpy(), sc.cpu().numpy()
-    # threshold polynomials (fit_threshold, peak_detection.py:89-109), one fit per width
-    ncoef = polydeg + 1
+    # threshold polynomials (fit_threshold, peak_detection.py:89-109), one fit per width:
+    # the fits of all trials with the same number of segments and all their widths in one
+    # stacked least-squares call
+    ncoef = int(polydeg) + 1
     coef = np.zeros((T, nw, ncoef), dtype=np.float64)
     polycos = [dict() for _ in range(T)]
+    nseg_t = np.diff(segoff.astype(np.int64))
+    by_nseg = {}
     for t in range(T):
-        a, b = int(segoff[t]), int(segoff[t + 1])
-        logfc = np.log(fc_h[a:b])
-        for iw in range(nw):
-            if b - a >= minseg:
-                c = np.poly1d(np.polyfit(logfc, sc_h[a:b, iw], polydeg)).coefficients
-            else:
-                c = np.array([smin], dtype=np.float64)
-            polycos[t][iw] = c if b - a >= minseg else [smin]
-            coef[t, iw, ncoef - len(c):] = c
+        if nseg_t[t] >= minseg:
+            by_nseg.setdefault(int(nseg_t[t]), []).append(t)
+        else:
+            for iw in range(nw):
+                polycos[t][iw] = [smin]
+                coef[t, iw, ncoef - 1] = smin
+    for M, ts in by_nseg.items():
+        X = np.stack([np.log(fc_h[int(segoff[t]):int(segoff[t + 1])]) for t in ts])
+        Y = np.stack([sc_h[int(segoff[t]):int(segoff[t + 1])].T for t in ts]).reshape(-1, M)
+        C = _polyfit_stacked(np.repeat(X, nw, axis=0), Y, polydeg)
+        for j, t in enumerate(ts):
+            for iw in range(nw):
+                c = np.poly1d(C[j * nw + iw]).coefficients
+                polycos[t][iw] = c
+                coef[t, iw, ncoef - len(c):] = c
     dcoef = torch.from_numpy(coef).to(p.device)
     sel = torch.empty(capacity, dtype=torch.int64, device=p.device)
     count = ctypes.c_size_t(0)

@@ -76,3 +76,51 @@ def test_search_then_peaks_on_device(rb):
             assert np.array_equal(np.asarray(polycos[iw], dtype=np.float64),
                                   np.asarray(refpc[iw], dtype=np.float64))
     bs.close()
+
+
+def _segment_case(rng, m, p, extra, T):
+    """A periodogram of m segments of p points (+ extra trailing points), frequencies
+    decreasing over (m - 0.5) segment widths, S/N with ties."""
+    w = 5.0 / T
+    n = m * p + extra
+    f = 3.0 - np.linspace(0.0, (m - 0.5) * w, n)
+    s = np.round(rng.standard_normal((n, 3)) * 2.0 + 5.0, 1).astype(np.float32)
+    return 1.0 / f, s
+
+
+@pytest.mark.parametrize("ps", [[3, 5, 64, 127], [129, 1000, 3000], [4312, 5000],
+                                [5, 129, 1000, 4312, 9000, 16000]])
+def test_peak_segments_sizes(rb, ps):
+    """rt_peak_segments against numpy's median / percentiles (the oracle's segment_stats) for
+    segments of 3 to 16000 points: every on-chip sort size (128 to 16384 values) and several
+    trials of different segment sizes in one launch."""
+    import ctypes
+
+    import torch
+
+    from riptide_b200 import _lib, libcpp
+
+    rng = np.random.default_rng(len(ps) * 7 + ps[0])
+    T = 100.0
+    cases = [_segment_case(rng, 11 + k, p, k % 3, T) for k, p in enumerate(ps)]
+    per = torch.from_numpy(np.concatenate([c[0] for c in cases])).cuda()
+    snr = torch.from_numpy(np.concatenate([c[1] for c in cases])).cuda()
+    rows = np.concatenate([[0], np.cumsum([c[0].size for c in cases])]).astype(np.uint64)
+    tobs = np.full(len(cases), T)
+    segoff = np.zeros(len(cases) + 1, dtype=np.uint64)
+    lib, dp = _lib.load(), ctypes.POINTER(ctypes.c_double)
+    args = (libcpp._ptr(per), None, 3, rows.ctypes.data_as(_lib._u64p), len(cases),
+            tobs.ctypes.data_as(dp), 5.0, 6.0, segoff.ctypes.data_as(_lib._u64p))
+    _lib.check(lib.rt_peak_segments(*args, None, None, libcpp._stream()))
+    fc = torch.empty(int(segoff[-1]), dtype=torch.float64, device="cuda")
+    sc = torch.empty((int(segoff[-1]), 3), dtype=torch.float64, device="cuda")
+    _lib.check(lib.rt_peak_segments(libcpp._ptr(per), libcpp._ptr(snr), *args[2:],
+                                    libcpp._ptr(fc), libcpp._ptr(sc), libcpp._stream()))
+    fc, sc = fc.cpu().numpy(), sc.cpu().numpy()
+    for t, (periods, s) in enumerate(cases):
+        a, b = int(segoff[t]), int(segoff[t + 1])
+        for iw in range(3):
+            f_ref, smed, sstd = O.segment_stats(1.0 / periods, s[:, iw], T)
+            assert b - a == f_ref.size
+            assert np.array_equal(fc[a:b], f_ref)
+            assert np.array_equal(sc[a:b, iw], smed + 6.0 * sstd), (t, iw)

@@ -232,3 +232,18 @@ def test_worker_pool_configuration():
                    [{"ffa_search": {"period_min": 1.0, "bogus": 1}, "find_peaks": {}}])
     with pytest.raises(ValueError, match="at least one"):
         WorkerPool({"rmed_width": 5.0, "rmed_minpts": 101}, [])
+
+
+def test_stacked_polyfit_is_np_polyfit():
+    """The threshold fits of find_peaks_batched, stacked into one least-squares call, return
+    exactly np.polyfit's coefficients (peak_detection.py:89-109 fits one width at a time)."""
+    from riptide_b200.peaks import _polyfit_stacked
+
+    rng = np.random.default_rng(11)
+    for M in (10, 47, 333):
+        X = np.sort(rng.uniform(-5.0, 3.0, (700, M)), axis=1)
+        Y = rng.standard_normal((700, M)) * 2.0 + 8.0
+        for deg in (2, 2.0, 3):
+            C = _polyfit_stacked(X, Y, deg)
+            R = np.array([np.polyfit(X[k], Y[k], deg) for k in range(X.shape[0])])
+            assert np.array_equal(C, R), (M, deg)
