@@ -12,8 +12,12 @@ Here a list of files is one batch:
   3. every further range searches those series (deredden=False, already_normalised=True);
   4. find_peaks runs batched over all trials of a range (peaks.find_peaks_batched).
 Trials are searched in chunks of `chunk_trials`, grouped by sampling time (a plan has one).
-Peaks come back in the reference's order: by file, then by range, then by decreasing S/N.
+The next chunk's files are read and copied to the device on a side stream by a loader thread
+while the current chunk is searched. Peaks come back in the reference's order: by file, then
+by range, then by decreasing S/N.
 """
+from concurrent.futures import ThreadPoolExecutor
+
 import numpy as np
 
 from . import libcpp
@@ -78,15 +82,36 @@ class WorkerPool(object):
 
     def process_fname_list(self, fnames):
         """Peaks of every file and range, flattened in the reference's order."""
+        torch = libcpp._t()
         files = describe(list(fnames), self.fmt)
         per_file = [[] for _ in files]
         groups = {}
         for i, f in enumerate(files):
             groups.setdefault(f.tsamp, []).append(i)
-        for tsamp, idx in groups.items():
-            for a in range(0, len(idx), self.chunk_trials):
-                chunk = idx[a:a + self.chunk_trials]
-                for i, peaks in zip(chunk, self._search_chunk([files[i] for i in chunk], tsamp)):
+        chunks = [(tsamp, idx[a:a + self.chunk_trials]) for tsamp, idx in groups.items()
+                  for a in range(0, len(idx), self.chunk_trials)]
+        if not chunks:
+            return []
+        main = torch.cuda.current_stream()
+        side = torch.cuda.Stream()
+
+        def load(chunk):
+            with torch.cuda.stream(side):
+                x, lengths = load_series_batch([files[i] for i in chunk[1]])
+                ev = torch.cuda.Event()
+                ev.record(side)
+            return x, lengths, ev
+
+        with ThreadPoolExecutor(1) as loader:
+            nxt = loader.submit(load, chunks[0])
+            for k, (tsamp, idx) in enumerate(chunks):
+                x, lengths, ev = nxt.result()
+                if k + 1 < len(chunks):
+                    nxt = loader.submit(load, chunks[k + 1])
+                main.wait_event(ev)
+                x.record_stream(main)
+                found = self._search_chunk(x, lengths, [files[i] for i in idx], tsamp)
+                for i, peaks in zip(idx, found):
                     per_file[i] = peaks
         return [p for plist in per_file for p in plist]
 
@@ -94,9 +119,8 @@ class WorkerPool(object):
         """Peaks of one file over every range (worker_pool.py:47-68)."""
         return self.process_fname_list([fname])
 
-    def _search_chunk(self, files, tsamp):
+    def _search_chunk(self, data, lengths, files, tsamp):
         torch = libcpp._t()
-        data, lengths = load_series_batch(files)
         tobs = lengths.astype(np.float64) * tsamp
         dms = [f.metadata.get("dm") for f in files]
         z = torch.empty_like(data)
