@@ -159,8 +159,11 @@ def measured_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def traffic_per_trial():
-    """DRAM bytes per trial of the search kernel from the committed ncu summary, or None."""
+def traffic_per_trial(config_id):
+    """DRAM bytes per trial of the search kernel from the committed ncu summary of this
+    workload (captured on the batched 2^22-sample configuration only), or None."""
+    if config_id != 3:
+        return None
     try:
         with open(os.path.join(HERE, "profiles", "search_persistent_traffic.json")) as f:
             return float(json.load(f)["dram_bytes_per_trial"])
@@ -288,7 +291,7 @@ def bench_ours(args):
     k_ms = stage[2] / args.steps
     peak, peak_kind = measured_peak()
     achieved = bytes_kernel / (k_ms * 1e-3) / 1e9
-    tr = traffic_per_trial()
+    tr = traffic_per_trial(args.config)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": (tr * ntrials if tr else None),
                 "kernel": "k_search_persistent", "peak_source": peak_kind,
