@@ -361,18 +361,27 @@ __global__ void __launch_bounds__(kDsThreads, 2)
     // Stage the segment + halo (and write the normalised copy if asked for). Warp w owns the
     // staged samples [w * kDsPerWarp, (w + 1) * kDsPerWarp), lane-strided so every shared
     // access is conflict-free.
+    // loads in batches of 8 per thread, all issued before any is used
     double wsum = 0.0;
+    constexpr int kBatch = 8;
+    static_assert(kDsChunks % kBatch == 0, "whole batches");
 #pragma unroll
-    for (int ch = 0; ch < kDsChunks; ++ch) {
-        const int i = warp * kDsPerWarp + ch * 32 + lane;
-        float x = 0.0f;
-        if (i < L) {
-            x = __ldg(z + i);
-            if (zout && i < seg)
-                zout[i] = __double2float_rn(__ddiv_rn(__dsub_rn((double)x, mean), inv));
+    for (int b0 = 0; b0 < kDsChunks; b0 += kBatch) {
+        float xb[kBatch];
+#pragma unroll
+        for (int q = 0; q < kBatch; ++q) {
+            const int i = warp * kDsPerWarp + (b0 + q) * 32 + lane;
+            xb[q] = (i < L) ? __ldg(z + i) : 0.0f;
         }
-        zs[i] = x;
-        wsum += (double)x;
+#pragma unroll
+        for (int q = 0; q < kBatch; ++q) {
+            const int i = warp * kDsPerWarp + (b0 + q) * 32 + lane;
+            const float x = xb[q];
+            if (zout && i < L && i < seg)
+                zout[i] = __double2float_rn(__ddiv_rn(__dsub_rn((double)x, mean), inv));
+            zs[i] = x;
+            wsum += (double)x;
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
