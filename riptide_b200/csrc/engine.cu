@@ -568,9 +568,7 @@ __global__ void __launch_bounds__(kStatThreads)
     const bool small = 2 * (unsigned long long)N < (1ull << 32);
     const double first = (k > 1) ? (double)fp[0] : 0.0;
     const double last = (k > 1) ? (double)fp[nl - 1] : 0.0;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N;
-         i += (size_t)blocks_per_trial * blockDim.x) {
-        const float xv = xr[i];
+    auto body = [&](size_t i, float xv) {
         float yv;
         if (k > 1) {
             const long long v = 2LL * (long long)i - (k - 1);
@@ -596,7 +594,19 @@ __global__ void __launch_bounds__(kStatThreads)
         const double d = (double)yv - shift_yd;
         s1 += d;
         s2 += d * d;
+    };
+    // four grid-stride steps per pass with their loads issued first; the sums keep the
+    // order of the plain loop
+    const size_t stride = (size_t)blocks_per_trial * blockDim.x;
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    for (; i + 3 * stride < N; i += 4 * stride) {
+        float xv[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) xv[q] = xr[i + q * stride];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) body(i + q * stride, xv[q]);
     }
+    for (; i < N; i += stride) body(i, xr[i]);
     // block reduction (fixed order)
     __shared__ double r1[kStatThreads], r2[kStatThreads];
     r1[threadIdx.x] = s1;
