@@ -224,9 +224,11 @@ void rt_search_plan_destroy(rt_search_plan* plan);
  * Host-buffer pipeline: the batched search of series in host memory, the way the
  * reference's worker pool searches DM trials from host memory (pipeline/worker_pool.py:35-68
  * calling search.py:11-93), with the copies in and out overlapped with the search. The
- * trials are cut into chunks of at most `chunk_trials` consecutive trials (one plan each);
- * while chunk i is searched, chunk i+1 is copied in and chunk i-1's periodograms are
- * copied out. Host buffers must be page-locked for the copies to overlap.
+ * trials are cut into chunks of at most `chunk_trials` consecutive trials (one plan each;
+ * the first and last chunks hold a quarter of that when there are enough trials, so that the
+ * copies that overlap no search are short); while chunk i is searched, chunk i+1 is copied
+ * in and chunk i-1's periodograms are copied out. Host buffers must be page-locked for the
+ * copies to overlap.
  * -------------------------------------------------------------------------------*/
 typedef struct rt_search_pipeline rt_search_pipeline;
 

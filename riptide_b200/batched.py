@@ -203,9 +203,9 @@ def _host_ptr(a, dtypes, n, name):
 class SearchPipeline(object):
     """Batched search of series held in host memory (C ABI rt_search_pipeline_*).
 
-    The trials are cut into chunks of ``chunk_trials`` consecutive trials; the copy of chunk
-    i+1 to the GPU and the copy of chunk i-1's periodograms back to the host overlap the
-    search of chunk i. Host buffers from ``allocate_host`` are page-locked, which the
+    The trials are cut into chunks of ``chunk_trials`` consecutive trials (a quarter of that
+    first and last, when there are enough trials); the copy of chunk i+1 to the GPU and the
+    copy of chunk i-1's periodograms back to the host overlap the search of chunk i. Host buffers from ``allocate_host`` are page-locked, which the
     overlap needs. Same outputs as ``BatchedSearch`` (every trial is searched independently).
     """
 

@@ -76,11 +76,29 @@ static int pipeline_build(rt_search_pipeline* P, const uint64_t* lengths, size_t
     P->nw = nw;
     RT_TRY_CUDA(cudaGetDevice(&P->device));
     P->rows.assign(ntrials + 1, 0);
-    size_t s = 0;
-    for (size_t t0 = 0; t0 < ntrials; t0 += chunk_trials) {
+    // chunk sizes: a quarter chunk first and last, so that the copy-in before the first
+    // search and the copy-out after the last one (the parts of the pipeline that overlap
+    // nothing) are short; full chunks in between
+    std::vector<size_t> sizes;
+    const size_t q = std::max<size_t>(1, chunk_trials / 4);
+    if (ntrials <= chunk_trials + 2 * q) {
+        for (size_t t0 = 0; t0 < ntrials; t0 += chunk_trials)
+            sizes.push_back(std::min(chunk_trials, ntrials - t0));
+    } else {
+        sizes.push_back(q);
+        size_t left = ntrials - 2 * q;
+        while (left > 0) {
+            const size_t n = std::min(chunk_trials, left);
+            sizes.push_back(n);
+            left -= n;
+        }
+        sizes.push_back(q);
+    }
+    size_t s = 0, t0 = 0;
+    for (size_t ci = 0; ci < sizes.size(); t0 += sizes[ci], ++ci) {
         Chunk c;
         c.t0 = t0;
-        c.nt = std::min(chunk_trials, ntrials - t0);
+        c.nt = sizes[ci];
         c.s0 = s;
         for (size_t i = 0; i < c.nt; ++i) s += lengths[t0 + i];
         c.ns = s - c.s0;

@@ -259,15 +259,16 @@ def test_batched_full_size_trial(rb):
 
 
 def test_pipeline_equals_batched(rb):
-    # host-buffer pipeline (3 chunks, so both device buffer pairs are reused) against the
-    # device-resident batched search of the same trials: identical outputs
+    # host-buffer pipeline (4 chunks of 1, 2, 1, 1 trials: quarter chunks first and last, both
+    # device buffer pairs reused) against the device-resident batched search of the same
+    # trials: identical outputs
     rng = np.random.default_rng(78)
     lengths = [70001, 65536, 90000, 50000, 81234]
     series = [rb.generate_signal(n, 0.9 / 5e-4 + 11 * i, ducy=0.04, amplitude=12.0, rng=rng)
               .astype(np.float32) + 0.25 for i, n in enumerate(lengths)]
     kw = dict(period_min=0.2, period_max=3.0, bins_min=240, bins_max=260, rmed_width=1.0)
     pipe = rb.SearchPipeline(lengths, 5e-4, chunk_trials=2, **kw)
-    assert pipe.num_chunks == 3
+    assert pipe.num_chunks == 4
     for _ in range(2):  # second run reuses every buffer and event
         pgs = pipe.search(series)
     ref = rb.ffa_search_batched(series, 5e-4, **kw)
