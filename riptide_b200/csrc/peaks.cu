@@ -108,6 +108,17 @@ __global__ void __launch_bounds__(1024)
         fc[seg] = (p & 1) ? sv[p / 2] : __ddiv_rn(__dadd_rn(sv[p / 2 - 1], sv[p / 2]), 2.0);
 }
 
+// First and last period of every trial's periodogram (the segment layout's frequency span).
+__global__ void k_period_ends(const double* __restrict__ periods,
+                              const unsigned long long* __restrict__ row_offsets, int ntrials,
+                              double* __restrict__ ends)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntrials) return;
+    ends[2 * t] = periods[row_offsets[t]];
+    ends[2 * t + 1] = periods[row_offsets[t + 1] - 1];
+}
+
 // Points above the dynamic threshold poly(log f) and above smin (find_peaks_single,
 // peak_detection.py:112-146), as (row * nw + iw), in any order.
 __global__ void k_peak_select(const double* __restrict__ periods, const float* __restrict__ snrs,
@@ -153,17 +164,33 @@ extern "C" int rt_peak_segments(const double* d_periods, const float* d_snrs, si
     if (!d_periods || !h_row_offsets || !h_tobs || !h_seg_offsets)
         return set_error(RT_EINVAL, "null argument");
     if (num_widths == 0 || num_widths > 65535) return set_error(RT_EINVAL, "bad number of widths");
-    // segment layout of every trial: m = ceil(|f[-1] - f[0]| / w), p = rows // m
+    // segment layout of every trial: m = ceil(|f[-1] - f[0]| / w), p = rows // m; the first
+    // and last period of every trial gathered on the device and copied back at once
+    if (ntrials == 0) return set_error(RT_EINVAL, "no periodograms");
+    for (size_t t = 0; t < ntrials; ++t)
+        if (h_row_offsets[t + 1] <= h_row_offsets[t])
+            return set_error(RT_EINVAL, "periodogram %zu is empty", t);
     std::vector<double> ends(2 * ntrials);
-    for (size_t t = 0; t < ntrials; ++t) {
-        const uint64_t a = h_row_offsets[t], b = h_row_offsets[t + 1];
-        if (b <= a) return set_error(RT_EINVAL, "periodogram %zu is empty", t);
-        RT_TRY_CUDA(cudaMemcpyAsync(&ends[2 * t], d_periods + a, sizeof(double),
-                                    cudaMemcpyDeviceToHost, st));
-        RT_TRY_CUDA(cudaMemcpyAsync(&ends[2 * t + 1], d_periods + b - 1, sizeof(double),
-                                    cudaMemcpyDeviceToHost, st));
+    {
+        unsigned long long* d_ro = nullptr;
+        double* d_ends = nullptr;
+        const size_t ro_bytes = (ntrials + 1) * sizeof(uint64_t);
+        const size_t ro_room = (ro_bytes + 15) & ~size_t(15);
+        RT_TRY_CUDA(cudaMallocAsync((void**)&d_ro, ro_room + 2 * ntrials * sizeof(double), st));
+        d_ends = reinterpret_cast<double*>(reinterpret_cast<char*>(d_ro) + ro_room);
+        cudaError_t e = cudaMemcpyAsync(d_ro, h_row_offsets, ro_bytes, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) {
+            k_period_ends<<<(unsigned)((ntrials + 255) / 256), 256, 0, st>>>(d_periods, d_ro,
+                                                                            (int)ntrials, d_ends);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(ends.data(), d_ends, 2 * ntrials * sizeof(double),
+                                cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        cudaFreeAsync(d_ro, st);
+        if (e != cudaSuccess) return check_cuda(e, "peak_segments layout");
     }
-    RT_TRY_CUDA(cudaStreamSynchronize(st));
     std::vector<SegTrial> tr(ntrials);
     uint64_t seg = 0, pmax = 1;
     h_seg_offsets[0] = 0;

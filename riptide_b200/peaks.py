@@ -149,11 +149,13 @@ def find_peaks_batched(periods, foldbins, snrs, row_offsets, tobs, widths, dms=N
         X = np.stack([np.log(fc_h[int(segoff[t]):int(segoff[t + 1])]) for t in ts])
         Y = np.stack([sc_h[int(segoff[t]):int(segoff[t + 1])].T for t in ts]).reshape(-1, M)
         C = _polyfit_stacked(np.repeat(X, nw, axis=0), Y, polydeg)
+        # np.poly1d(c).coefficients: leading zeros trimmed, [0.] when all are zero
+        lead = np.argmax(C != 0, axis=1)
+        lead[~(C != 0).any(axis=1)] = ncoef - 1
+        coef[ts] = C.reshape(len(ts), nw, ncoef)
         for j, t in enumerate(ts):
             for iw in range(nw):
-                c = np.poly1d(C[j * nw + iw]).coefficients
-                polycos[t][iw] = c
-                coef[t, iw, ncoef - len(c):] = c
+                polycos[t][iw] = C[j * nw + iw, lead[j * nw + iw]:]
     dcoef = torch.from_numpy(coef).to(p.device)
     sel = torch.empty(capacity, dtype=torch.int64, device=p.device)
     count = ctypes.c_size_t(0)
