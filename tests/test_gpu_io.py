@@ -155,3 +155,43 @@ def test_worker_pool_matches_reference(tmp_path):
     assert np.allclose([p.snr for p in peaks], g["snr"], rtol=1e-5)
     assert np.allclose([p.period for p in peaks], g["period"], rtol=1e-12)
     assert [(p.iw, p.ip, p.snr) for p in single] == [(p.iw, p.ip, p.snr) for p in peaks]
+
+
+def test_worker_pool_sigproc_8bit_equals_float(tmp_path):
+    """8-bit SIGPROC files (payload copied as bytes, widened on the GPU) give the same peaks as
+    float32 PRESTO files holding the same values."""
+    from riptide_b200 import WorkerPool, generate_signal
+    from riptide_b200.reading.writers import write_presto, write_sigproc
+
+    rng = np.random.default_rng(21)
+    tsamp, n = 1e-3, 150000
+    ranges = [{"ffa_search": {"period_min": 0.5, "period_max": 5.0, "bins_min": 240,
+                              "bins_max": 260}, "find_peaks": {"smin": 6.0}}]
+    dered = {"rmed_width": 4.0, "rmed_minpts": 101}
+    tims, infs = [], []
+    for i, signed in enumerate((True, False, True)):
+        x = generate_signal(n, (0.7 + 0.3 * i) / tsamp, ducy=0.03, amplitude=25.0, rng=rng)
+        v = np.clip(np.round(x * 12.0) + (0 if signed else 128), -128 if signed else 0,
+                    127 if signed else 255)
+        hdr = dict(source_name="fake", telescope_id=4, machine_id=10, data_type=2,
+                   refdm=float(i), fch1=1400.0, nchans=1, nbits=8, signed=signed,
+                   tstart=60000.0, tsamp=tsamp, nifs=1, src_raj=0.0, src_dej=0.0)
+        fn = str(tmp_path / f"t{i}.tim")
+        write_sigproc(fn, v, hdr)
+        tims.append(fn)
+        base = str(tmp_path / f"p{i}")
+        write_presto(base, v.astype(np.float32), dict(
+            basename=f"p{i}", telescope="Parkes", instrument="x", source_name="fake",
+            raj="00:00:00.0000", decj="00:00:00.0000", observer="x", mjd=60000.0,
+            barycentered=False, nsamp=n, tsamp=tsamp, breaks=False, em_band="Radio",
+            fov_arcsec=1.0, dm=float(i), fbot=1200.0, bandwidth=400.0, nchan=1, cbw=1.0,
+            analyst="x"))
+        infs.append(base + ".inf")
+    a = WorkerPool(dered, ranges, fmt="sigproc", chunk_trials=2)
+    b = WorkerPool(dered, ranges, fmt="presto", chunk_trials=2)
+    try:
+        pa, pb = a.process_fname_list(tims), b.process_fname_list(infs)
+    finally:
+        a.close()
+        b.close()
+    assert pa and [(p.iw, p.ip, p.snr, p.dm) for p in pa] == [(p.iw, p.ip, p.snr, p.dm) for p in pb]
