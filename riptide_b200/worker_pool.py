@@ -13,8 +13,9 @@ Here a list of files is one batch:
   4. find_peaks runs batched over all trials of a range (peaks.find_peaks_batched).
 Trials are searched in chunks of `chunk_trials`, grouped by sampling time (a plan has one).
 The next chunk's files are read and copied to the device on a side stream by a loader thread
-while the current chunk is searched. Peaks come back in the reference's order: by file, then
-by range, then by decreasing S/N.
+while the current chunk is searched, and a finder thread runs find_peaks on the previous
+chunk's periodograms (on a stream of its own) while the next one is searched. Peaks come back
+in the reference's order: by file, then by range, then by decreasing S/N.
 """
 from concurrent.futures import ThreadPoolExecutor
 
@@ -102,7 +103,9 @@ class WorkerPool(object):
                 ev.record(side)
             return x, lengths, ev
 
-        with ThreadPoolExecutor(1) as loader:
+        finder_stream = torch.cuda.Stream()
+        pending = []
+        with ThreadPoolExecutor(1) as loader, ThreadPoolExecutor(1) as finder:
             nxt = loader.submit(load, chunks[0])
             for k, (tsamp, idx) in enumerate(chunks):
                 x, lengths, ev = nxt.result()
@@ -110,8 +113,14 @@ class WorkerPool(object):
                     nxt = loader.submit(load, chunks[k + 1])
                 main.wait_event(ev)
                 x.record_stream(main)
-                found = self._search_chunk(x, lengths, [files[i] for i in idx], tsamp)
-                for i, peaks in zip(idx, found):
+                chunk_files = [files[i] for i in idx]
+                searched = self._search_chunk(x, lengths, tsamp)
+                done = torch.cuda.Event()
+                done.record(main)
+                pending.append((idx, finder.submit(self._peaks_chunk, searched, done,
+                                                   finder_stream, lengths, chunk_files, tsamp)))
+            for idx, fut in pending:
+                for i, peaks in zip(idx, fut.result()):
                     per_file[i] = peaks
         return [p for plist in per_file for p in plist]
 
@@ -119,22 +128,36 @@ class WorkerPool(object):
         """Peaks of one file over every range (worker_pool.py:47-68)."""
         return self.process_fname_list([fname])
 
-    def _search_chunk(self, data, lengths, files, tsamp):
+    def _search_chunk(self, data, lengths, tsamp):
+        """Every range's periodograms of one chunk, in output tensors of this chunk's own."""
+        torch = libcpp._t()
+        z = torch.empty_like(data)
+        searched = []
+        for r in range(len(self.range_confs)):
+            bs = self._plan(r, lengths, tsamp)
+            outs = bs.allocate_outputs(data.device)
+            if r == 0:
+                bs.run(data, outs, normalised=z)
+            else:
+                bs.run(z, outs)
+            searched.append((bs.row_offsets, bs.widths, outs))
+        return searched
+
+    def _peaks_chunk(self, searched, done, stream, lengths, files, tsamp):
+        """find_peaks of every range of one chunk, on `stream` after the event `done`."""
         torch = libcpp._t()
         tobs = lengths.astype(np.float64) * tsamp
         dms = [f.metadata.get("dm") for f in files]
-        z = torch.empty_like(data)
         out = [[] for _ in files]
-        for r, conf in enumerate(self.range_confs):
-            bs = self._plan(r, lengths, tsamp)
-            if r == 0:
-                periods, foldbins, snrs = bs.run(data, normalised=z)
-            else:
-                periods, foldbins, snrs = bs.run(z)
-            res = find_peaks_batched(periods, foldbins, snrs, bs.row_offsets, tobs, bs.widths,
-                                     dms=dms, **dict(conf.get("find_peaks") or {}))
-            for t, (peaks, _) in enumerate(res):
-                out[t].append(peaks)
+        with torch.cuda.stream(stream):
+            stream.wait_event(done)
+            for (rows, widths, outs), conf in zip(searched, self.range_confs):
+                for t in outs:
+                    t.record_stream(stream)
+                res = find_peaks_batched(outs[0], outs[1], outs[2], rows, tobs, widths,
+                                         dms=dms, **dict(conf.get("find_peaks") or {}))
+                for t, (peaks, _) in enumerate(res):
+                    out[t].append(peaks)
         return [[p for plist in ranges for p in plist] for ranges in out]
 
     def close(self):
