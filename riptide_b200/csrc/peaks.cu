@@ -12,7 +12,8 @@
 
 namespace rt {
 
-constexpr int kSegMaxPoints = 16384;  // points per segment, sorted on chip
+constexpr int kSegMaxPoints = 16384;       // points per segment, sorted on chip
+constexpr size_t kSegColsSmem = 112 * 1024;  // shared memory of the all-widths segment kernel
 
 // In-place ascending bitonic sort of n (a power of two) values in shared memory. Each
 // compare-exchange stage is n/2 independent pairs (i, i + j), i with bit j clear, dealt to
@@ -104,6 +105,73 @@ __global__ void __launch_bounds__(1024)
         sv[i] = (i < p) ? __ddiv_rn(1.0, periods[r0 + i]) : INFINITY;
     __syncthreads();
     bitonic_sort(sv, n2);
+    if (threadIdx.x == 0)  // np.median: the middle value, or the mean of the middle two
+        fc[seg] = (p & 1) ? sv[p / 2] : __ddiv_rn(__dadd_rn(sv[p / 2 - 1], sv[p / 2]), 2.0);
+}
+
+// In-place ascending bitonic sorts of `ncols` columns of n values each (column c at a + c*n),
+// all columns advancing through the same network together: more independent
+// compare-exchanges per thread and per barrier than one column at a time.
+template <typename T>
+__device__ void bitonic_sort_cols(T* a, int n, int ncols)
+{
+    const int half = n >> 1;
+    int lh = 0;
+    while ((1 << lh) < half) ++lh;
+    for (int k = 2; k <= n; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int q = threadIdx.x; q < ncols * half; q += blockDim.x) {
+                const int col = q >> lh, qq = q & (half - 1);
+                const int i = ((qq & ~(j - 1)) << 1) | (qq & (j - 1));
+                T* c = a + (size_t)col * n;
+                const bool up = (i & k) == 0;
+                const T x = c[i], y = c[i + j];
+                if ((x > y) == up) {
+                    c[i] = y;
+                    c[i + j] = x;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// One CTA per segment for every width at once: the segment's nw S/N columns sorted together
+// (float32), then its frequencies (float64); the same statistics as k_peak_segments.
+__global__ void __launch_bounds__(512)
+    k_peak_segments_cols(const double* __restrict__ periods, const float* __restrict__ snrs,
+                         int nw, const SegTrial* __restrict__ trials, int ntrials, double nstd,
+                         int n2, double* __restrict__ fc, double* __restrict__ sc)
+{
+    extern __shared__ double sv[];                        // n2 frequencies
+    float* vf = reinterpret_cast<float*>(sv + n2);        // nw columns of n2 S/N values
+    const int seg = blockIdx.x;
+    int lo = 0, hi = ntrials - 1;  // trial of this segment
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (trials[mid].seg0 <= seg) lo = mid;
+        else hi = mid - 1;
+    }
+    const SegTrial T = trials[lo];
+    const int j = seg - T.seg0, p = T.p;
+    const size_t r0 = T.row0 + (size_t)j * p;
+    for (int e = threadIdx.x; e < nw * n2; e += blockDim.x) {
+        const int i = e / nw, iw = e - i * nw;  // row-major reads of the periodogram
+        if (i < n2) vf[(size_t)iw * n2 + i] = (i < p) ? snrs[(r0 + i) * nw + iw] : INFINITY;
+    }
+    for (int i = threadIdx.x; i < n2; i += blockDim.x)
+        sv[i] = (i < p) ? __ddiv_rn(1.0, periods[r0 + i]) : INFINITY;
+    __syncthreads();
+    bitonic_sort_cols(vf, n2, nw);
+    bitonic_sort_cols(sv, n2, 1);
+    for (int iw = threadIdx.x; iw < nw; iw += blockDim.x) {
+        const float* c = vf + (size_t)iw * n2;
+        const double s25 = np_percentile_sorted(c, p, 0.25);
+        const double s50 = np_percentile_sorted(c, p, 0.5);
+        const double s75 = np_percentile_sorted(c, p, 0.75);
+        const double sstd = __ddiv_rn(__dsub_rn(s75, s25), 1.349);
+        sc[(size_t)seg * nw + iw] = __dadd_rn(s50, __dmul_rn(nstd, sstd));
+    }
     if (threadIdx.x == 0)  // np.median: the middle value, or the mean of the middle two
         fc[seg] = (p & 1) ? sv[p / 2] : __ddiv_rn(__dadd_rn(sv[p / 2 - 1], sv[p / 2]), 2.0);
 }
@@ -232,7 +300,22 @@ extern "C" int rt_peak_segments(const double* d_periods, const float* d_snrs, si
                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)(kSegMaxPoints * sizeof(double))),
                        "peak_segments");
-    if (s == RT_OK && seg > 0) {
+    // all widths of a segment in one CTA when they fit two CTAs per SM's shared memory
+    const size_t smem_cols = (size_t)n2 * (sizeof(double) + num_widths * sizeof(float));
+    if (s == RT_OK && seg > 0 && smem_cols <= kSegColsSmem) {
+        if (smem_cols > 48 * 1024)
+            s = check_cuda(cudaFuncSetAttribute(k_peak_segments_cols,
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)kSegColsSmem),
+                           "peak_segments");
+        if (s == RT_OK) {
+            const int tc = (int)std::max<size_t>(
+                32, std::min<size_t>(512, (num_widths * (size_t)n2 / 2 + 31) / 32 * 32));
+            k_peak_segments_cols<<<(unsigned)seg, tc, smem_cols, st>>>(
+                d_periods, d_snrs, (int)num_widths, d_tr, (int)ntrials, nstd, n2, d_fc, d_sc);
+            s = check_cuda(cudaGetLastError(), "peak_segments");
+        }
+    } else if (s == RT_OK && seg > 0) {
         dim3 grid((unsigned)seg, (unsigned)num_widths);
         k_peak_segments<<<grid, threads, smem, st>>>(d_periods, d_snrs, (int)num_widths, d_tr,
                                                      (int)ntrials, nstd, n2, d_fc, d_sc);
