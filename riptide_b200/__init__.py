@@ -6,7 +6,7 @@ reference's Python API on top. ``riptide_b200.libcpp`` replaces ``riptide.libcpp
 from . import libcpp
 from .batched import BatchedSearch, SearchPipeline, ffa_search_batched
 from .ffautils import generate_width_trials
-from .folding import fold, fold_batched
+from .folding import fold, fold_batched, fold_candidates
 from .libffa import boxcar_snr, downsample, ffa1, ffa2, ffafreq, ffaprd, generate_signal
 from .metadata import Metadata
 from .peaks import Peak, find_peaks, find_peaks_batched
@@ -21,5 +21,5 @@ __all__ = [
     "ffa1",
     "ffa2", "ffafreq", "ffaprd", "generate_signal", "downsample", "boxcar_snr",
     "running_median", "fast_running_median", "generate_width_trials", "libcpp",
-    "find_peaks", "find_peaks_batched", "Peak", "fold", "fold_batched", "Metadata", "WorkerPool",
+    "find_peaks", "find_peaks_batched", "Peak", "fold", "fold_batched", "fold_candidates", "Metadata", "WorkerPool",
 ]

@@ -70,3 +70,19 @@ def fold(ts, period, bins, subints=None):
     (subints, bins) sub-integrations, all full periods when subints is None, or one profile of
     `bins` values when subints == 1. ValueError for the reference's invalid arguments."""
     return fold_batched(ts, [period], int(bins), subints)[0]
+
+
+def candidate_subints(period, subints, length):
+    """The sub-integrations a pipeline candidate is folded with (candidate.py:76-104): the
+    requested number, or None (every full period in the data) when that many periods do not
+    fit in the series."""
+    if subints is not None and subints * period >= length:
+        return None
+    return subints
+
+
+def fold_candidates(ts, periods, bins, subints=1):
+    """Fold one TimeSeries at every candidate period in one launch, with the candidate stage's
+    rule for sub-integrations (candidate_subints). Returns the list of folded arrays."""
+    subs = [candidate_subints(float(p), subints, ts.length) for p in np.asarray(periods).ravel()]
+    return fold_batched(ts, periods, bins, subs)

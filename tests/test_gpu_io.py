@@ -101,6 +101,21 @@ def test_fold_batched_equals_single_folds():
         assert np.array_equal(y, ts.fold(p, 128, subints=s))
 
 
+def test_fold_candidates_rule():
+    """Candidate folding (candidate.py:76-104): every period folded with the requested
+    sub-integrations, or all full periods where that many do not fit."""
+    from riptide_b200 import TimeSeries, fold_candidates
+
+    x = np.random.default_rng(9).standard_normal(100000).astype(np.float32)
+    ts = TimeSeries(x, 1e-4)  # 10 s
+    periods = [0.25, 0.5, 1.0, 3.0]
+    got = fold_candidates(ts, periods, 64, subints=16)
+    for p, y in zip(periods, got):
+        want = ts.fold(p, 64, subints=None if 16 * p >= ts.length else 16)
+        assert np.array_equal(y, want)
+    assert got[0].shape == (16, 64) and got[2].shape == (10, 64)
+
+
 def test_fold_reference_methods():
     """tests/test_time_series.py:106-204 of the reference (the folding part)."""
     from riptide_b200 import TimeSeries

@@ -247,3 +247,18 @@ def test_stacked_polyfit_is_np_polyfit():
             C = _polyfit_stacked(X, Y, deg)
             R = np.array([np.polyfit(X[k], Y[k], deg) for k in range(X.shape[0])])
             assert np.array_equal(C, R), (M, deg)
+
+
+def test_candidate_subints_rule():
+    """candidate.py:76-104: subints falls back to None when that many periods exceed the data."""
+    from riptide_b200.folding import candidate_subints, fold_shape
+
+    length = 10.0
+    assert candidate_subints(1.0, 32, length) is None
+    assert candidate_subints(0.25, 32, length) == 32
+    assert candidate_subints(0.3125, 32, length) is None  # 32 periods == the data length
+    assert candidate_subints(2.0, None, length) is None
+    assert candidate_subints(2.0, 1, length) == 1
+    # the folded shapes the candidate stage gets for a 10 s series at 1 ms
+    assert fold_shape(10000, 1e-3, 1.0, 100, candidate_subints(1.0, 32, length)) == (10, 100)
+    assert fold_shape(10000, 1e-3, 0.25, 100, candidate_subints(0.25, 32, length)) == (32, 100)
