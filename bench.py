@@ -358,6 +358,10 @@ def bench_ours(args):
     if args.workerpool > 0 and rank == 0:
         wp_line = bench_workerpool(args, cfg, data, lengths, pool if do_cpu else None)
 
+    # ---- readers and candidate folding (opt-in) ----
+    io_line = bench_ingest(args, cfg, data, lengths) if args.ingest > 0 and rank == 0 else None
+    fold_line = bench_fold(args, cfg, data, lengths) if args.fold > 0 and rank == 0 else None
+
     # ---- plain per-(cycle, bins) GPU path on a few trials, for the batching ratio ----
     plain = None
     if rank == 0 and args.plain_trials > 0:
@@ -418,6 +422,8 @@ def bench_ours(args):
             "batched_vs_plain": (value / world / plain["trials_per_s"]) if plain else None,
             "find_peaks": peaks_line,
             "workerpool": wp_line,
+            "ingest": io_line,
+            "fold": fold_line,
         }
         print(json.dumps(line), flush=True)
     bs.close()
@@ -491,6 +497,96 @@ def bench_workerpool(args, cfg, data, lengths, pool):
         shutil.rmtree(tmp, ignore_errors=True)
 
 
+def bench_ingest(args, cfg, data, lengths):
+    """Time load_series_batch on `args.ingest` SIGPROC files of the workload, float32 and
+    8-bit (written first, read from the page cache), against the reference's data path for
+    the same files (np.fromfile + astype(np.float32) per file, one core, then one copy of
+    the packed batch to the GPU)."""
+    import shutil
+    import tempfile
+
+    import torch
+
+    from riptide_b200.reading import describe, load_series_batch
+    from riptide_b200.reading.writers import write_sigproc
+
+    n = min(int(args.ingest), len(lengths))
+    offs = np.concatenate([[0], np.cumsum(lengths)])
+    tmp = tempfile.mkdtemp(prefix="rt_io_")
+    out = {}
+    try:
+        for nbits in (32, 8):
+            fnames = []
+            for i in range(n):
+                x = data[int(offs[i]):int(offs[i + 1])].cpu().numpy()
+                if nbits == 8:
+                    x = np.clip(np.round(x * 16.0), -128, 127)
+                hdr = dict(source_name="synthetic", telescope_id=0, machine_id=0, data_type=2,
+                           refdm=float(i), fch1=1400.0, nchans=1, nbits=nbits, tstart=60000.0,
+                           tsamp=cfg["tsamp"], nifs=1, src_raj=0.0, src_dej=0.0)
+                if nbits == 8:
+                    hdr["signed"] = True
+                fn = os.path.join(tmp, f"t{i:04d}_{nbits}.tim")
+                write_sigproc(fn, x, hdr)
+                fnames.append(fn)
+            files = describe(fnames, "sigproc")
+            load_series_batch(files)
+            torch.cuda.synchronize()
+            best = 1e30
+            for _ in range(3):
+                t0 = time.perf_counter()
+                dev, _ = load_series_batch(files)
+                torch.cuda.synchronize()
+                best = min(best, time.perf_counter() - t0)
+            t0 = time.perf_counter()
+            host = [np.fromfile(f.path, dtype=(np.float32 if nbits == 32 else np.int8),
+                                offset=f.offset).astype(np.float32) for f in files]
+            torch.from_numpy(np.concatenate(host)).to("cuda")
+            torch.cuda.synchronize()
+            ref = time.perf_counter() - t0
+            payload = sum(f.nsamp for f in files) * (4 if nbits == 32 else 1)
+            out[f"nbits{nbits}"] = {"files": n, "s": best, "files_per_s": n / best,
+                                    "payload_GB_per_s": payload / best / 1e9,
+                                    "reference_path_files_per_s": n / ref}
+        return out
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+def bench_fold(args, cfg, data, lengths):
+    """Fold trial 0 at `args.fold` candidate periods (log-uniform over the search range,
+    256 bins, 32 sub-integrations with the candidate rule) in one fold_candidates call, against
+    the reference's TimeSeries.fold arithmetic on the host (the oracle's restatement: numpy and
+    the C restatement of downsample.hpp, one core) on a sample of 32 of them."""
+    import torch
+
+    import riptide_b200 as rb
+    from oracle import oracle as O
+
+    x = data[:int(lengths[0])].cpu().numpy()
+    ts = rb.TimeSeries(x, cfg["tsamp"])
+    rng = np.random.default_rng(5)
+    lo, hi = np.log(cfg["search"]["period_min"]), np.log(cfg["search"]["period_max"])
+    periods = np.exp(rng.uniform(lo, hi, int(args.fold)))
+    rb.fold_candidates(ts, periods[:8], 256, 32)
+    best = 1e30
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rb.fold_candidates(ts, periods, 256, 32)
+        torch.cuda.synchronize()
+        best = min(best, time.perf_counter() - t0)
+    sample = periods[:32]
+    t0 = time.perf_counter()
+    for p in sample:
+        sub = rb.folding.candidate_subints(float(p), 32, ts.length)
+        O.fold(x, cfg["tsamp"], float(p), 256, sub)
+    cpu = (time.perf_counter() - t0) / len(sample)
+    return {"candidates": int(args.fold), "s_all": best, "ms_per_candidate": best * 1e3 / args.fold,
+            "cpu_ms_per_candidate_1_core": cpu * 1e3, "cpu_kind": "port",
+            "api": "fold_candidates (rt_fold_batched, one launch), host series copied in"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -508,6 +604,10 @@ def main():
     ap.add_argument("--peaks", action="store_true")
     ap.add_argument("--workerpool", type=int, default=0,
                     help="also time WorkerPool.process_fname_list on this many files")
+    ap.add_argument("--ingest", type=int, default=0,
+                    help="also time load_series_batch on this many SIGPROC files")
+    ap.add_argument("--fold", type=int, default=0,
+                    help="also time fold_candidates at this many candidate periods")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
