@@ -355,3 +355,26 @@ def test_tuned_engine_is_bit_identical(rb):
     best = TU.autotune(lengths, 64e-6, sample_trials=2, repeats=1, **kw)
     assert best in TU.candidates(260)
     assert TU.autotune(lengths, 64e-6, sample_trials=2, repeats=1, **kw) == best  # cached
+
+
+@pytest.mark.parametrize("config_id", [2, 5])
+def test_survey_configurations_full_size(rb, config_id):
+    """One full-size series of the single survey-length configuration (2^23 samples, white +
+    1/f noise, three pulsars, P 0.2-60 s) and of the large sweep's generator (2^23 samples,
+    bins 480-520, 12 widths), through the batched engine, against the
+    reference's own libcpp periodogram (the oracle's glue for deredden and normalise; the C
+    restatement where the reference could not be built)."""
+    from riptide_b200 import synth
+
+    cfg = synth.CONFIGS[config_id]
+    n = int(synth.trial_lengths(config_id, 1, 0)[0])
+    x, _ = synth.make_trial(config_id, 0, n, cfg["tsamp"], "cuda")
+    x = x.cpu().numpy()
+    kw = dict(cfg["search"])
+    bs = rb.BatchedSearch([n], cfg["tsamp"], **kw)
+    pgs, zs = bs.search([x], return_normalised=True)
+    bs.close()
+    z, widths, p, fb, sn = O.ffa_search(x, cfg["tsamp"], libcpp=O.ref_libcpp(), **kw)
+    assert np.array_equal(pgs[0].widths, widths)
+    assert np.allclose(zs[0], z, rtol=1e-5, atol=1e-5)
+    _check_pgram(pgs[0].periods, pgs[0].foldbins, pgs[0].snrs, p, fb, sn, rtol=1e-4, atol=1e-4)
