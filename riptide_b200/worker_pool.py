@@ -95,9 +95,10 @@ class WorkerPool(object):
             return []
         main = torch.cuda.current_stream()
         side = torch.cuda.Stream()
+        dev = torch.cuda.current_device()  # the helper threads work on the caller's device
 
         def load(chunk):
-            with torch.cuda.stream(side):
+            with torch.cuda.device(dev), torch.cuda.stream(side):
                 x, lengths = load_series_batch([files[i] for i in chunk[1]])
                 ev = torch.cuda.Event()
                 ev.record(side)
@@ -117,7 +118,7 @@ class WorkerPool(object):
                 searched = self._search_chunk(x, lengths, tsamp)
                 done = torch.cuda.Event()
                 done.record(main)
-                pending.append((idx, finder.submit(self._peaks_chunk, searched, done,
+                pending.append((idx, finder.submit(self._peaks_chunk, searched, done, dev,
                                                    finder_stream, lengths, chunk_files, tsamp)))
             for idx, fut in pending:
                 for i, peaks in zip(idx, fut.result()):
@@ -143,13 +144,14 @@ class WorkerPool(object):
             searched.append((bs.row_offsets, bs.widths, outs))
         return searched
 
-    def _peaks_chunk(self, searched, done, stream, lengths, files, tsamp):
-        """find_peaks of every range of one chunk, on `stream` after the event `done`."""
+    def _peaks_chunk(self, searched, done, dev, stream, lengths, files, tsamp):
+        """find_peaks of every range of one chunk, on device `dev` and `stream`, after the
+        event `done`."""
         torch = libcpp._t()
         tobs = lengths.astype(np.float64) * tsamp
         dms = [f.metadata.get("dm") for f in files]
         out = [[] for _ in files]
-        with torch.cuda.stream(stream):
+        with torch.cuda.device(dev), torch.cuda.stream(stream):
             stream.wait_event(done)
             for (rows, widths, outs), conf in zip(searched, self.range_confs):
                 for t in outs:
