@@ -156,14 +156,18 @@ int rt_search_plan_create(const uint64_t* h_lengths, size_t ntrials,
                           const rt_search_config* cfg, const uint64_t* h_widths,
                           size_t num_widths, rt_search_plan** plan);
 /* Engine tile choices (0 = default), as picked by an autotuner:
- *   rows_fraction  rows per job as a fraction (0, 1] of what the shared memory holds;
- *   snr_threads    threads per profile in the S/N: 8 (bins <= 264 only) or 16;
- *   lag_items      work items between two stages of a multi-stage transform (default 640).
+ *   rows_fraction       rows per job as a fraction (0, 1] of what the shared memory holds,
+ *                       for transforms of up to 8 jobs' worth of rows;
+ *   snr_threads         threads per profile in the S/N: 8 (bins <= 264 only) or 16;
+ *   lag_items           work items between two stages of a multi-stage transform (640);
+ *   rows_fraction_deep  the same fraction for transforms of more rows than that (0: the
+ *                       value of rows_fraction).
  * Results do not depend on these; only the speed does. No counterpart in the reference. */
 typedef struct rt_search_tuning {
     double rows_fraction;
     int snr_threads;
     int lag_items;
+    double rows_fraction_deep;
 } rt_search_tuning;
 int rt_search_plan_create_tuned(const uint64_t* h_lengths, size_t ntrials,
                                 const rt_search_config* cfg, const uint64_t* h_widths,

@@ -103,7 +103,7 @@ class PlanStats(ctypes.Structure):
 
 class SearchTuning(ctypes.Structure):
     _fields_ = [("rows_fraction", ctypes.c_double), ("snr_threads", ctypes.c_int),
-                ("lag_items", ctypes.c_int)]
+                ("lag_items", ctypes.c_int), ("rows_fraction_deep", ctypes.c_double)]
 
 
 class SearchTransform(ctypes.Structure):

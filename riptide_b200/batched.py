@@ -20,7 +20,8 @@ class BatchedSearch(object):
                  bins_max=260, ducy_max=0.20, wtsp=1.5, deredden=True, rmed_width=4.0,
                  rmed_minpts=101, already_normalised=False, widths=None, tuning=None):
         """`tuning`: engine tile choices, a dict with any of rows_fraction, snr_threads,
-        lag_items (riptide_b200.tuning.autotune picks them); results do not depend on it."""
+        lag_items, rows_fraction_deep (riptide_b200.tuning.autotune picks them); results do
+        not depend on it."""
         self.lengths = np.ascontiguousarray(np.asarray(lengths, dtype=np.uint64).ravel())
         self.tsamp = float(tsamp)
         self.widths = (np.asarray(widths) if widths is not None
@@ -38,7 +39,8 @@ class BatchedSearch(object):
         if tuning:
             tn = _lib.SearchTuning(rows_fraction=float(tuning.get("rows_fraction", 0.0)),
                                    snr_threads=int(tuning.get("snr_threads", 0)),
-                                   lag_items=int(tuning.get("lag_items", 0)))
+                                   lag_items=int(tuning.get("lag_items", 0)),
+                                   rows_fraction_deep=float(tuning.get("rows_fraction_deep", 0.0)))
             _lib.check(_lib.load().rt_search_plan_create_tuned(
                 lp, self.lengths.size, ctypes.byref(cfg), wp, w.size, ctypes.byref(tn),
                 ctypes.byref(h)))

@@ -738,7 +738,7 @@ __global__ void k_normalise(const float* __restrict__ x, TrialArrays A, const do
 struct SearchPlan {
     // configuration
     rt_search_config cfg;
-    rt_search_tuning tuning = {1.0, 0, 0};
+    rt_search_tuning tuning = {1.0, 0, 0, 0.0};
     std::vector<int> widths;
     int nfast = 0;
     std::vector<size_t> lengths, offsets;
@@ -901,9 +901,13 @@ static int plan_build(SearchPlan& P)
                 if (re == 0) continue;
                 if (rows >= (1u << 24))
                     return set_error(RT_EINVAL, "transform of %zu rows is too large", rows);
-                // rows per job: the shared-memory capacity, scaled by the tuning
-                const double frac = P.tuning.rows_fraction > 0 ? std::min(1.0, P.tuning.rows_fraction) : 1.0;
-                const int capr = std::max(4, (int)((double)engine_cap_rows((int)b) * frac));
+                // rows per job: the shared-memory capacity, scaled by the tuning (its own
+                // fraction for transforms of more than 8 jobs' worth of rows)
+                const int cap_full = engine_cap_rows((int)b);
+                double frac = P.tuning.rows_fraction > 0 ? std::min(1.0, P.tuning.rows_fraction) : 1.0;
+                if (rows > 8 * (size_t)cap_full && P.tuning.rows_fraction_deep > 0)
+                    frac = std::min(1.0, P.tuning.rows_fraction_deep);
+                const int capr = std::max(4, (int)((double)cap_full * frac));
                 // S/N threads per profile: 8 where the register window allows it, unless tuned
                 const int tpr = (P.tuning.snr_threads == 16) ? 16 : snr_tpr((int)b);
                 const auto key = std::make_pair((int)rows, (long long)re * 8192 + (long long)b);
@@ -1585,6 +1589,8 @@ extern "C" int rt_search_plan_create_tuned(const uint64_t* lengths, size_t ntria
 {
     if (tuning && !(tuning->rows_fraction >= 0.0 && tuning->rows_fraction <= 1.0))
         return set_error(RT_EINVAL, "rows_fraction must be in [0, 1]");
+    if (tuning && !(tuning->rows_fraction_deep >= 0.0 && tuning->rows_fraction_deep <= 1.0))
+        return set_error(RT_EINVAL, "rows_fraction_deep must be in [0, 1]");
     if (tuning && tuning->snr_threads != 0 && tuning->snr_threads != 8 && tuning->snr_threads != 16)
         return set_error(RT_EINVAL, "snr_threads must be 0, 8 or 16");
     if (tuning && tuning->lag_items < 0) return set_error(RT_EINVAL, "lag_items must be >= 0");

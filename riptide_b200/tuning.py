@@ -1,16 +1,20 @@
 """Autotuner of the engine's tile choices.
 
-The persistent search kernel has three choices that change its speed but not its results
-(rt_search_tuning):
-  rows_fraction  rows per job, as a fraction of what shared memory holds: fewer rows make
-                 more, smaller jobs (less cone recomputation per job, more per-job overhead);
-  snr_threads    threads per profile in the S/N (8 or 16): more threads per profile finish
-                 a job's last, partial round of profiles sooner;
-  lag_items      work items between two stages of a multi-stage transform: a longer lag
-                 leaves the previous stage more time to finish (fewer waits), a shorter one
-                 keeps its output in L2.
+The persistent search kernel has choices that change its speed but not its results
+(rt_search_tuning), made per transform from its rows (m) and bins (b):
+  rows_fraction       rows per job, as a fraction of what shared memory holds at this b:
+                      fewer rows make more, smaller jobs (less cone recomputation per job,
+                      more per-job overhead);
+  rows_fraction_deep  the same for the transforms of more than 8 jobs' worth of rows, the ones
+                      cut into several stages;
+  snr_threads         threads per profile in the S/N (8 or 16; 8 only for b <= 264): more
+                      threads per profile finish a job's last, partial round sooner;
+  lag_items           work items between two stages of a multi-stage transform: a longer lag
+                      leaves the previous stage more time to finish (fewer waits), a shorter
+                      one keeps its output in L2.
 `autotune` times the engine on a sample of the workload (synthetic noise of the same
-lengths, the same search parameters) for a small grid of candidates and returns the fastest,
+lengths, the same search parameters): first a grid of rows_fraction x snr_threads x
+lag_items, then rows_fraction_deep around the best of the grid. It returns the fastest,
 caching the answer per (search parameters, lengths) for the process and, optionally, in a
 JSON file.
 """
@@ -19,7 +23,8 @@ import os
 
 import numpy as np
 
-DEFAULT = {"rows_fraction": 1.0, "snr_threads": 0, "lag_items": 0}
+DEFAULT = {"rows_fraction": 1.0, "snr_threads": 0, "lag_items": 0, "rows_fraction_deep": 0.0}
+DEEP_FRACTIONS = (0.9, 0.8, 0.7)
 
 
 def candidates(bins_max):
@@ -29,7 +34,8 @@ def candidates(bins_max):
     for rf in (1.0, 0.9, 0.8):
         for tpr in tprs:
             for lag in (0, 320, 1280):
-                out.append({"rows_fraction": rf, "snr_threads": tpr, "lag_items": lag})
+                out.append({"rows_fraction": rf, "snr_threads": tpr, "lag_items": lag,
+                            "rows_fraction_deep": 0.0})
     return out
 
 
@@ -90,11 +96,18 @@ def autotune(lengths, tsamp, sample_trials=16, repeats=3, cache_file=None, verbo
     gen.manual_seed(12345)
     data = torch.randn(int(sum(sample)), generator=gen, device="cuda", dtype=torch.float32)
     results = []
-    for cand in candidates(int(search_kw.get("bins_max", 260))):
+
+    def trial(cand):
         ms = time_search(sample, tsamp, cand, data, repeats=repeats, **search_kw)
         results.append((ms, cand))
         if verbose:
             print("autotune %s: %.3f ms" % (cand, ms), flush=True)
+
+    for cand in candidates(int(search_kw.get("bins_max", 260))):
+        trial(cand)
+    grid_best = min(results, key=lambda r: r[0])[1]
+    for fd in DEEP_FRACTIONS:  # the deep transforms' own rows per job, around the grid's best
+        trial(dict(grid_best, rows_fraction_deep=fd))
     results.sort(key=lambda r: r[0])
     best = results[0][1]
     _CACHE[key] = best

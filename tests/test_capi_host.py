@@ -98,6 +98,18 @@ def test_tuned_plan_checks_and_shapes():
     finally:
         base.close()
         tuned.close()
-    for bad in ({"rows_fraction": 1.5}, {"snr_threads": 12}, {"lag_items": -1}):
+    # rows_fraction_deep applies only to transforms of more than 8 jobs' worth of rows: a
+    # smaller value cuts those into more jobs, but fewer than the same fraction everywhere
+    plans = [BatchedSearch([2 ** 22], 64e-6, tuning=t, **kw)
+             for t in ({"rows_fraction": 1.0}, {"rows_fraction_deep": 0.6}, {"rows_fraction": 0.6})]
+    try:
+        items = [p.stats["num_work_items"] for p in plans]
+        assert all(np.array_equal(plans[0].row_offsets, p.row_offsets) for p in plans)
+        assert items[0] < items[1] < items[2], items
+    finally:
+        for p in plans:
+            p.close()
+    for bad in ({"rows_fraction": 1.5}, {"snr_threads": 12}, {"lag_items": -1},
+                {"rows_fraction_deep": -0.1}):
         with pytest.raises(ValueError):
             BatchedSearch([100000], 1e-3, period_min=0.5, period_max=2.0, tuning=bad)

@@ -353,8 +353,21 @@ def test_tuned_engine_is_bit_identical(rb):
             assert torch.equal(a, b), tun
         bs.close()
     best = TU.autotune(lengths, 64e-6, sample_trials=2, repeats=1, **kw)
-    assert best in TU.candidates(260)
+    grid = TU.candidates(260)
+    assert best in grid or (best["rows_fraction_deep"] in TU.DEEP_FRACTIONS
+                            and dict(best, rows_fraction_deep=0.0) in grid)
     assert TU.autotune(lengths, 64e-6, sample_trials=2, repeats=1, **kw) == best  # cached
+    # a 2^22-sample series has transforms of more than 8 jobs' worth of rows, which the deep
+    # fraction cuts into more jobs: the same periodogram
+    y = torch.from_numpy(rng.standard_normal(1 << 22).astype(np.float32)).cuda()
+    kw = dict(period_min=0.2, period_max=30.0)
+    a = rb.BatchedSearch([1 << 22], 64e-6, **kw)
+    b = rb.BatchedSearch([1 << 22], 64e-6, tuning={"rows_fraction_deep": 0.5}, **kw)
+    assert b.stats["num_work_items"] > a.stats["num_work_items"]
+    for u, v in zip(a.run(y), b.run(y)):
+        assert torch.equal(u, v)
+    a.close()
+    b.close()
 
 
 @pytest.mark.parametrize("config_id", [2, 5])
