@@ -38,12 +38,12 @@ __device__ void bitonic_sort(T* a, int n)
     }
 }
 
-// numpy's linear interpolation between two order statistics (numpy _lerp): the difference
-// b - a is taken in the input's type, float32 for S/N values (exact operands: the sorted
-// values are float32 values held in doubles), the rest in float64.
-__device__ __forceinline__ double np_lerp_f32(double a, double b, double t)
+// numpy's linear interpolation between two order statistics (numpy _lerp) of float64
+// values: the reference takes the percentiles of each width's S/N after casting them to
+// float64 (peak_detection.py:205), so the difference b - a is a float64 one.
+__device__ __forceinline__ double np_lerp(double a, double b, double t)
 {
-    const double d = (double)__fsub_rn((float)b, (float)a);
+    const double d = __dsub_rn(b, a);
     return (t >= 0.5) ? __dsub_rn(b, __dmul_rn(d, __dsub_rn(1.0, t))) : __dadd_rn(a, __dmul_rn(d, t));
 }
 
@@ -60,7 +60,8 @@ struct SegTrial {
 template <typename T>
 __device__ __forceinline__ double np_percentile_sorted(const T* a, int n, double q);
 
-// np.percentile(x, q) of n sorted float32 values, method 'linear'
+// np.percentile(x, q), method 'linear', of n sorted float32 S/N values cast to float64 (their
+// order is the same either way)
 template <>
 __device__ __forceinline__ double np_percentile_sorted<float>(const float* a, int n, double q)
 {
@@ -68,7 +69,7 @@ __device__ __forceinline__ double np_percentile_sorted<float>(const float* a, in
     const double prev = floor(v);
     const int i0 = (int)prev;
     const int i1 = min(i0 + 1, n - 1);
-    return np_lerp_f32(a[i0], a[i1], __dsub_rn(v, prev));
+    return np_lerp((double)a[i0], (double)a[i1], __dsub_rn(v, prev));
 }
 
 __global__ void __launch_bounds__(1024)

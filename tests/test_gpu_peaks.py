@@ -120,7 +120,8 @@ def test_peak_segments_sizes(rb, ps):
     for t, (periods, s) in enumerate(cases):
         a, b = int(segoff[t]), int(segoff[t + 1])
         for iw in range(3):
-            f_ref, smed, sstd = O.segment_stats(1.0 / periods, s[:, iw], T)
+            # the reference casts each width's S/N to float64 first (peak_detection.py:205)
+            f_ref, smed, sstd = O.segment_stats(1.0 / periods, s[:, iw].astype(float), T)
             assert b - a == f_ref.size
             assert np.array_equal(fc[a:b], f_ref)
             assert np.array_equal(sc[a:b, iw], smed + 6.0 * sstd), (t, iw)
