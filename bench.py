@@ -362,27 +362,15 @@ def bench_ours(args):
     io_line = bench_ingest(args, cfg, data, lengths) if args.ingest > 0 and rank == 0 else None
     fold_line = bench_fold(args, cfg, data, lengths) if args.fold > 0 and rank == 0 else None
 
-    # ---- plain per-(cycle, bins) GPU path on a few trials, for the batching ratio ----
-    plain = None
-    if rank == 0 and args.plain_trials > 0:
-        offs = np.concatenate([[0], np.cumsum(lengths)])
-        tms = []
-        for i in range(args.plain_trials):
-            x = data[int(offs[i]):int(offs[i + 1])]
-            t1 = time.perf_counter()
-            y = torch.empty_like(x)
-            z = torch.empty_like(x)
-            p = rb.libcpp
-            _lib.check(_lib.load().rt_deredden(p._ptr(x), x.numel(), cfg["tsamp"],
-                                               cfg["search"]["rmed_width"],
-                                               cfg["search"]["rmed_minpts"], p._ptr(y), p._stream()))
-            _lib.check(_lib.load().rt_normalise(p._ptr(y), y.numel(), p._ptr(z), p._stream()))
-            rb.libcpp.periodogram_plain(z, cfg["tsamp"], bs.widths, cfg["search"]["period_min"],
-                                        cfg["search"]["period_max"], cfg["search"]["bins_min"],
-                                        cfg["search"]["bins_max"])
-            torch.cuda.synchronize()
-            tms.append(time.perf_counter() - t1)
-        plain = {"trials_per_s": 1.0 / float(np.median(tms)), "sample_trials": args.plain_trials}
+    # ---- plain per-trial GPU paths on a few trials, for the batching ratio ----
+    plain = bench_plain(args, cfg, data, lengths) if rank == 0 and args.plain_trials > 0 else None
+    # ---- the large-sweep workload and the differentiable search (rank 0, default on) ----
+    sweep = bench_sweep(args) if rank == 0 and args.sweep_trials > 0 else None
+    grad_line = None
+    if rank == 0 and not args.no_grad:
+        from riptide_b200.grad import benchmark_training_step
+
+        grad_line = benchmark_training_step(64, steps=3, warmup=2)
 
     # ---- CPU baseline (rank 0, N = 1) ----
     cpu = None
@@ -404,6 +392,8 @@ def bench_ours(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded white + 1/f noise + von Mises pulsars, generated on device)",
             "config": {"workload": cfg["name"], "trials_per_gpu": ntrials,
+                       "period_range_s": [cfg["search"]["period_min"], cfg["search"]["period_max"]],
+                       "bins": [cfg["search"]["bins_min"], cfg["search"]["bins_max"]],
                        "samples_per_gpu": int(sum(lengths)), "periodogram_rows_per_gpu": L,
                        "widths": nw, "l2": "inputs larger than L2 (%.1f GB per step)" %
                        (4 * sum(lengths) / 1e9),
@@ -419,7 +409,12 @@ def bench_ours(args):
             "clocks": clocks,
             "cpu_baseline": cpu,
             "plain_gpu": plain,
-            "batched_vs_plain": (value / world / plain["trials_per_s"]) if plain else None,
+            "batched_vs_plain": (value / world / plain["engine_one_trial"]["trials_per_s"])
+            if plain else None,
+            "batched_vs_per_launch": (value / world / plain["per_launch"]["trials_per_s"])
+            if plain and plain.get("per_launch") else None,
+            "large_sweep": sweep,
+            "grad": grad_line,
             "find_peaks": peaks_line,
             "workerpool": wp_line,
             "ingest": io_line,
@@ -432,6 +427,118 @@ def bench_ours(args):
 
         dist.destroy_process_group()
     return 0
+
+
+def _event_ms(fn, reps):
+    """Mean CUDA-event time (ms) of fn() over reps calls on the current stream."""
+    import torch
+
+    st = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(st)
+    for _ in range(reps):
+        fn()
+    b.record(st)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def bench_plain(args, cfg, data, lengths):
+    """The per-trial GPU paths the batched engine replaces, on the first `plain_trials`
+    trials of the workload:
+    * engine_one_trial: the fused engine searching one trial per run (BatchedSearch of one
+      trial = rt_periodogram's path: deredden, normalise, downsampling, the persistent
+      FFA + S/N kernel), plans built outside the timed region, CUDA events over 3 runs;
+    * per_launch: rt_deredden + rt_normalise + rt_periodogram_plain (one launch per (cycle,
+      bins) step), on 2 trials."""
+    import torch
+
+    import riptide_b200 as rb
+    from riptide_b200 import _lib
+
+    offs = np.concatenate([[0], np.cumsum(lengths)])
+    n_eng = min(args.plain_trials, len(lengths))
+    ms = []
+    for i in range(n_eng):
+        x = data[int(offs[i]):int(offs[i + 1])]
+        one = rb.BatchedSearch([lengths[i]], cfg["tsamp"], **cfg["search"])
+        outs = one.allocate_outputs()
+        one.run(x, outs, check=True)
+        ms.append(_event_ms(lambda: one.run(x, outs, check=False), 3))
+        one.close()
+        del outs
+    eng = {"trials_per_s": 1e3 / float(np.mean(ms)), "ms_per_trial": float(np.mean(ms)),
+           "sample_trials": n_eng,
+           "api": "BatchedSearch of one trial per run (deredden, normalise, downsampling, "
+                  "persistent FFA + S/N kernel), CUDA events"}
+    per_launch = None
+    n_pl = min(2, len(lengths))
+    if n_pl:
+        tms = []
+        p = rb.libcpp
+        for i in range(n_pl):
+            x = data[int(offs[i]):int(offs[i + 1])]
+            y = torch.empty_like(x)
+            z = torch.empty_like(x)
+
+            def run():
+                _lib.check(_lib.load().rt_deredden(p._ptr(x), x.numel(), cfg["tsamp"],
+                                                   cfg["search"]["rmed_width"],
+                                                   cfg["search"]["rmed_minpts"], p._ptr(y),
+                                                   p._stream()))
+                _lib.check(_lib.load().rt_normalise(p._ptr(y), y.numel(), p._ptr(z), p._stream()))
+                from riptide_b200.ffautils import generate_width_trials
+
+                w = generate_width_trials(cfg["search"]["bins_min"])
+                p.periodogram_plain(z, cfg["tsamp"], w, cfg["search"]["period_min"],
+                                    cfg["search"]["period_max"], cfg["search"]["bins_min"],
+                                    cfg["search"]["bins_max"])
+
+            run()
+            tms.append(_event_ms(run, 1))
+        per_launch = {"trials_per_s": 1e3 / float(np.mean(tms)), "sample_trials": n_pl,
+                      "api": "rt_deredden + rt_normalise + rt_periodogram_plain (one launch per "
+                             "(cycle, bins) step)"}
+    return {"engine_one_trial": eng, "per_launch": per_launch}
+
+
+def bench_sweep(args):
+    """The large batched sweep's workload (2^23-sample trials, 64 us, P 0.2-60 s, bins
+    480-520, 12 widths) on `sweep_trials` trials in one batch: trials/s with inputs in HBM
+    (graph replays, CUDA events) and the search kernel's HBM roofline fraction."""
+    import torch
+
+    import riptide_b200 as rb
+    from riptide_b200 import _lib, synth
+
+    cfg = synth.CONFIGS[5]
+    data, lengths, _ = synth.make_batch(5, args.sweep_trials)
+    bs = rb.BatchedSearch(lengths, cfg["tsamp"], **cfg["search"])
+    st = bs.stats
+    nw = int(bs.widths.size)
+    bytes_kernel = 4 * st["folded_samples"] + st["total_rows"] * (4 * nw + 12)
+    outs = bs.allocate_outputs()
+    bs.run(data, outs, check=True)
+    bs.enable_graph(True)
+    bs.run(data, outs, check=False)
+    steps = 3
+    ms = _event_ms(lambda: bs.run(data, outs, check=False), steps)
+    _lib.check(_lib.load().rt_search_check(bs._plan, rb.libcpp._stream()))
+    bs.enable_timing(True)
+    bs.run(data, outs, check=True)
+    s0, s1, s2, _ = bs.last_timing()
+    bs.close()
+    peak, kind = measured_peak()
+    achieved = bytes_kernel / (s2 * 1e-3) / 1e9
+    del data, outs
+    torch.cuda.empty_cache()
+    return {"workload": cfg["name"], "trials": args.sweep_trials, "steps": steps,
+            "value": args.sweep_trials / (ms * 1e-3), "unit": "trials/s", "ms_per_step": ms,
+            "stage_ms": {"deredden_normalise": s0, "downsample": s1, "ffa_snr": s2},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "kernel": "k_search_persistent",
+                         "peak_source": kind, "alg_bytes_per_launch": bytes_kernel}}
 
 
 def bench_workerpool(args, cfg, data, lengths, pool):
@@ -596,7 +703,12 @@ def main():
     ap.add_argument("--config", type=int, default=3, choices=[1, 2, 3, 5])
     ap.add_argument("--trials", type=int, default=None)
     ap.add_argument("--cpu-sample", type=int, default=64)
-    ap.add_argument("--plain-trials", type=int, default=2)
+    ap.add_argument("--plain-trials", type=int, default=8,
+                    help="trials timed one at a time through the fused engine")
+    ap.add_argument("--sweep-trials", type=int, default=64,
+                    help="trials of the large-sweep workload timed beside the main line (0: skip)")
+    ap.add_argument("--no-grad", action="store_true",
+                    help="skip the differentiable-search training step")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--chunk-trials", type=int, default=32)
     ap.add_argument("--no-graph", action="store_true")

@@ -222,6 +222,22 @@ int rt_search_last_timing(rt_search_plan* plan, float* h_ms, int* h_launches);
  * 15 items of stages after the first. */
 int rt_search_set_profiling(rt_search_plan* plan, int enable);
 int rt_search_phase_cycles(rt_search_plan* plan, uint64_t* h_counters16, int reset);
+/* Bound of every wait inside the search kernel (a later stage of a transform waiting for
+ * the earlier one, a transform waiting for its scratch slot), in polls with a backoff of up
+ * to ~1 us between polls; default 20,000,000. A wait that runs out makes every CTA leave and
+ * the run report RT_ETIMEOUT (rt_search_check); the context stays usable. No counterpart in
+ * the reference, whose search has no device waits. */
+int rt_search_set_wait_limit(rt_search_plan* plan, long long polls);
+/* Host-side fault injection for tests of the error paths (no GPU fault is raised):
+ * RT_FAULT_STAGE_WAIT: later-stage work items wait for one job more than their previous
+ * stage has, a count that is never reached, so the run ends with RT_ETIMEOUT after the wait
+ * limit; RT_FAULT_ALLOC: the plan's device buffers are released and allocation number `arg`
+ * (from 1) of the next run fails with RT_ENOMEM (everything allocated before it is released
+ * again); RT_FAULT_NONE clears both. No counterpart in the reference. */
+#define RT_FAULT_NONE 0
+#define RT_FAULT_STAGE_WAIT 1
+#define RT_FAULT_ALLOC 2
+int rt_search_inject_fault(rt_search_plan* plan, int kind, int arg);
 void rt_search_plan_destroy(rt_search_plan* plan);
 
 /* ---------------------------------------------------------------------------------

@@ -9,9 +9,10 @@ Two checkers live here:
 * ``C``      -- ctypes binding of ``riptide_oracle.c`` (a restatement of the reference's
                C++ headers, cpp/*.hpp, float32 and FP64 variants).
 * ``ref_libcpp()`` -- the reference's own pybind11 module ``libcpp`` compiled from its
-               sources by ``oracle/Makefile`` into ``oracle/_ref/`` (present when the
-               reference was available at build time; the built file travels with the
-               repository snapshot).
+               sources by ``oracle/Makefile`` (target ``ref``, run by the build entry point
+               where the reference sources are present) into ``oracle/_ref/``. The built
+               module is not committed; it exists in a working tree where that build ran,
+               and is None elsewhere.
 
 and a numpy restatement of the Python glue around them: ``generate_width_trials``
 (ffautils.py:4-11), ``scrunch`` / ``fast_running_median`` (running_medians.py:40-85),

@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(HERE, "_riptide_b200.so")
 
 RT_OK, RT_EINVAL, RT_ECUDA, RT_ENOMEM, RT_ETIMEOUT, RT_EINTERNAL, RT_EIO = 0, 1, 2, 3, 4, 5, 6
 RT_SAMPLES_F32, RT_SAMPLES_U8, RT_SAMPLES_I8 = 0, 1, 2
+RT_FAULT_NONE, RT_FAULT_STAGE_WAIT, RT_FAULT_ALLOC = 0, 1, 2
 
 _sz = ctypes.c_size_t
 _vp = ctypes.c_void_p
@@ -52,6 +53,8 @@ SIGNATURES = {
     "rt_search_set_profiling": (ctypes.c_int, [_vp, ctypes.c_int]),
     "rt_search_phase_cycles": (ctypes.c_int, [_vp, _u64p, ctypes.c_int]),
     "rt_search_plan_destroy": (None, [_vp]),
+    "rt_search_set_wait_limit": (ctypes.c_int, [_vp, ctypes.c_longlong]),
+    "rt_search_inject_fault": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
     "rt_search_plan_prepare": (ctypes.c_int, [_vp]),
     "rt_search_plan_transforms": (ctypes.c_int, [_vp, _vp]),
     "rt_search_normalisation": (ctypes.c_int, [_vp, ctypes.POINTER(_d), ctypes.POINTER(_d), _vp]),

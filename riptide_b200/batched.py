@@ -162,6 +162,21 @@ class BatchedSearch(object):
                  "levels_run", "root_rows", "later_stage_items"]
         return {n: int(c[i]) for i, n in enumerate(names)}
 
+    def set_wait_limit(self, polls):
+        """Bound of the waits inside the search kernel, in polls (default 20,000,000). A wait
+        that runs out ends the run with RT_ETIMEOUT instead of hanging."""
+        _lib.check(_lib.load().rt_search_set_wait_limit(self._plan, int(polls)))
+
+    def inject_fault(self, kind, arg=0):
+        """Host-side fault injection for tests of the error paths (no GPU fault is raised):
+        "stage_wait" makes later-stage work items wait on a count that is never reached (the
+        run ends with RT_ETIMEOUT after the wait limit); "alloc" releases the plan's device
+        buffers and makes allocation number `arg` of the next run fail (RT_ENOMEM); None
+        clears both."""
+        kinds = {None: _lib.RT_FAULT_NONE, "stage_wait": _lib.RT_FAULT_STAGE_WAIT,
+                 "alloc": _lib.RT_FAULT_ALLOC}
+        _lib.check(_lib.load().rt_search_inject_fault(self._plan, kinds[kind], int(arg)))
+
     def close(self):
         if getattr(self, "_plan", None):
             _lib.load().rt_search_plan_destroy(self._plan)

@@ -56,7 +56,7 @@ RT_HD int engine_cap_rows(int b)
 
 constexpr int kSlots = 256;          // scratch slots for multi-stage transforms
 constexpr size_t kLagItems = 640;    // work items emitted between two stages of a transform
-constexpr long long kSpinLimit = 20000000LL;  // bounded waits (about 2-20 s with backoff)
+constexpr long long kSpinLimit = 20000000LL;  // default bound of the waits (about 2-20 s with backoff)
 
 struct EngineArgs {
     const float* ds;         // downsampled series arena
@@ -72,11 +72,14 @@ struct EngineArgs {
     int nw, nfast;
     float* scratch;          // kSlots * 2 * slot_floats
     size_t slot_floats;
-    int* done;               // [nseq * kMaxStages]
+    int* done;               // [nseq * kMaxStages]: jobs of the stage, once all are finished
+    int* fin;                // [nseq * kMaxStages]: jobs of the stage finished so far
     int* slot_release;       // [kSlots]
     unsigned long long* ticket;
     int* error;              // RT_OK or an error code
     unsigned long long* phase_cycles;  // optional [kPhases] SM-cycle totals (thread 0 of each CTA)
+    long long spin_limit;    // polls before a wait gives up with RT_ETIMEOUT
+    int dep_bias;            // added to later-stage dependency targets (fault injection; 0)
 };
 
 // Phases of one work item, for the optional in-kernel profile.
@@ -90,21 +93,6 @@ __device__ __forceinline__ int ld_acquire(const int* p)
     int v;
     asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
-}
-
-// Bounded wait until *p >= target. Returns false (and records RT_ETIMEOUT) on timeout or if
-// another CTA already failed.
-__device__ bool wait_at_least(const int* p, int target, int* error)
-{
-    unsigned ns = 32;
-    for (long long it = 0; it < kSpinLimit; ++it) {
-        if (ld_acquire(p) >= target) return true;
-        if (ld_acquire(error) != RT_OK) return false;
-        __nanosleep(ns);
-        if (ns < 1024) ns <<= 1;
-    }
-    atomicExch(error, RT_ETIMEOUT);
-    return false;
 }
 
 template <int TPR>
@@ -167,20 +155,39 @@ __device__ __forceinline__ unsigned warps_done_acquire(const unsigned* counter)
     return v;
 }
 
-// Completion of an item for the other CTAs: its stage counter and, after the last job of the
-// last stage, the release of the transform's scratch slot. Called by one thread after every
-// compute warp of the CTA has released the item (CTA scope); the fence makes their global
-// writes visible at GPU scope before the counters.
+// Drops the L2 lines wholly inside [p, p + bytes) without writing them back to DRAM (their
+// contents become undefined).
+__device__ __forceinline__ void discard_l2(const void* p, size_t bytes)
+{
+    uintptr_t a = ((uintptr_t)p + 127) & ~uintptr_t(127);
+    const uintptr_t e = ((uintptr_t)p + bytes) & ~uintptr_t(127);
+    for (; a < e; a += 128) asm volatile("discard.global.L2 [%0], 128;" ::"l"(a) : "memory");
+}
+
+// Completion of an item for the other CTAs. Called by one thread after every compute warp of
+// the CTA has released the item (CTA scope); the fence makes their global writes visible at
+// GPU scope before the counters. The job that finishes its stage last (the `fin` count)
+// publishes the stage: its input, the previous stage's output in the scratch ring, is read
+// by nobody any more, so its L2 lines are dropped unwritten (otherwise every stage output
+// would be written back to DRAM when L2 evicts it, although it is consumed from L2); then
+// the stage count (`done`, which the next stage waits for) or, after the last stage, the
+// transform's scratch slot is released. The discards precede the release, so no later
+// writer of that memory can race with them.
 __device__ __forceinline__ void signal_item_done(const EngineArgs& A, const ItemSlot& P)
 {
     if (P.X.seq < 0 || !P.done_ok) return;
     __threadfence();
-    int* d = A.done + (size_t)P.X.seq * kMaxStages + P.stage;
-    const int prev = atomicAdd(d, 1);
-    if (P.last && prev + 1 == P.jobs_of_stage) {
+    const size_t k = (size_t)P.X.seq * kMaxStages + P.stage;
+    const int prev = atomicAdd(A.fin + k, 1);
+    if (prev + 1 != P.jobs_of_stage) return;
+    if (P.stage > 0) {
+        const float* in = A.scratch + (size_t)(P.X.seq % kSlots) * 2 * A.slot_floats +
+                          (size_t)((P.stage - 1) & 1) * A.slot_floats;
+        discard_l2(in, (size_t)P.X.m * ffa_stride(P.X.b) * sizeof(float));
         __threadfence();
-        atomicAdd(A.slot_release + (P.X.seq % kSlots), 1);
     }
+    if (P.last) atomicAdd(A.slot_release + (P.X.seq % kSlots), 1);
+    else atomicAdd(A.done + k, P.jobs_of_stage);
 }
 
 // Scheduler-side view of a claimed item: its slot contents and its dependency.
@@ -220,7 +227,7 @@ __device__ void sched_decode(const EngineArgs& A, long long t, SchedItem& it)
             it.target = seq / kSlots;
         } else {
             it.dep = A.done + (size_t)seq * kMaxStages + stage - 1;
-            it.target = P.jobs[stage - 1];
+            it.target = P.jobs[stage - 1] + A.dep_bias;
         }
     }
 }
@@ -295,7 +302,7 @@ __device__ void scheduler_warp(const EngineArgs& A, ItemSlot* slots, JobTree* tr
                     chosen = true;
                     break;
                 }
-                if (spin > kSpinLimit) {
+                if (spin > A.spin_limit) {
                     atomicExch(A.error, RT_ETIMEOUT);
                     L.ticket = A.nitems;
                     L.ok = 0;
@@ -467,24 +474,163 @@ struct TrialArrays {
     const size_t* lo_off;    // [T] offsets into the packed scrunched series
 };
 
-// lores[j] = float32 mean of x[j*k .. (j+1)*k) (running_medians.py:40-46). One warp per value.
-__global__ void k_scrunch(const float* __restrict__ x, TrialArrays A, int k,
+// ---- numpy's pairwise summation -----------------------------------------------------
+// The reference's scrunch is `data[:N].reshape(-1, k).mean(axis=1)` on float32 data
+// (running_medians.py:40-46). numpy reduces each contiguous row with its pairwise sum in the
+// input type (numpy/_core/src/umath/loops_utils.h.src, pairwise_sum): a block of n < 8
+// values is summed in turn from -0.0; a block of 8 <= n <= 128 values in eight strided
+// accumulators r[j] = a[j] + a[j+8] + ... over its first n - n%8 values, combined as
+// ((r0+r1)+(r2+r3))+((r4+r5)+(r6+r7)), with the n%8 trailing values then added in turn; a
+// longer block is split at n2 = n/2 - (n/2)%8 and the two halves' sums are added. The mean is
+// that float32 sum divided by k, correctly rounded (numpy divides in float64 and casts; a
+// float64 quotient of float32 operands rounds to float32 exactly as a float32 division).
+// Reproduced here in the same order, so the scrunched series is bit-identical.
+constexpr int kPwLeaf = 128;
+
+// Leaves (blocks of <= 128 values) of the recursion over n values, left to right.
+static int pw_num_leaves(long long n)
+{
+    if (n <= kPwLeaf) return 1;
+    long long n2 = n / 2;
+    n2 -= n2 % 8;
+    return pw_num_leaves(n2) + pw_num_leaves(n - n2);
+}
+
+// Fills leaves[] with (start, length) in recursion (left to right) order; explicit stack.
+__device__ void pw_leaf_table(int n, int2* leaves)
+{
+    int st_s[40], st_n[40];
+    int sp = 0, nl = 0;
+    st_s[sp] = 0;
+    st_n[sp++] = n;
+    while (sp > 0) {
+        --sp;
+        const int s = st_s[sp], m = st_n[sp];
+        if (m <= kPwLeaf) {
+            leaves[nl++] = make_int2(s, m);
+            continue;
+        }
+        int m2 = m / 2;
+        m2 -= m2 % 8;
+        // right half pushed first, so the left half is popped (and emitted) first
+        st_s[sp] = s + m2;
+        st_n[sp++] = m - m2;
+        st_s[sp] = s;
+        st_n[sp++] = m2;
+    }
+}
+
+// Adds the leaf sums up the recursion tree of n values in numpy's order (left + right at
+// every split); leaf sums are consumed left to right.
+__device__ float pw_combine(const float* leaf_sums, int n)
+{
+    int fn[40], fstate[40];
+    float fleft[40];
+    int sp = 0, li = 0;
+    float ret = 0.0f;
+    fn[0] = n;
+    fstate[0] = 0;
+    sp = 1;
+    while (sp > 0) {
+        const int t = sp - 1;
+        const int m = fn[t];
+        if (m <= kPwLeaf) {
+            ret = leaf_sums[li++];
+            --sp;
+            continue;
+        }
+        int m2 = m / 2;
+        m2 -= m2 % 8;
+        if (fstate[t] == 0) {  // descend left
+            fstate[t] = 1;
+            fn[sp] = m2;
+            fstate[sp++] = 0;
+        } else if (fstate[t] == 1) {  // left done: descend right
+            fleft[t] = ret;
+            fstate[t] = 2;
+            fn[sp] = m - m2;
+            fstate[sp++] = 0;
+        } else {  // both done
+            ret = __fadd_rn(fleft[t], ret);
+            --sp;
+        }
+    }
+    return ret;
+}
+
+// lores[j] = float32 mean of x[j*k .. (j+1)*k), numpy's pairwise order (see above).
+// One warp per scrunched value; the warp's four 8-lane groups take one leaf each, a lane
+// one of the eight strided accumulators; lane 0 adds the leaf sums up the tree.
+// Dynamic shared memory: the leaf table (int2 per leaf) and one leaf-sum row per warp.
+__global__ void k_scrunch(const float* __restrict__ x, TrialArrays A, int k, int nleaves,
                           float* __restrict__ lores)
 {
+    extern __shared__ __align__(16) unsigned char sm_scrunch[];
+    int2* leaves = reinterpret_cast<int2*>(sm_scrunch);
+    float* sums = reinterpret_cast<float*>(leaves + nleaves) + (threadIdx.x >> 5) * nleaves;
+    if (threadIdx.x == 0) pw_leaf_table(k, leaves);
+    __syncthreads();
     const int trial = blockIdx.y;
     const size_t nl = A.lo_len[trial];
     const float* xr = x + A.off[trial];
     float* o = lores + A.lo_off[trial];
     const int lane = threadIdx.x & 31;
+    const int grp = lane >> 3, c = lane & 7;
     const size_t w0 = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
     const size_t nwarp = ((size_t)gridDim.x * blockDim.x) >> 5;
     for (size_t j = w0; j < nl; j += nwarp) {
-        double acc = 0.0;
-        for (int i = lane; i < k; i += 32) acc += (double)__ldg(xr + j * k + i);
-#pragma unroll
-        for (int o2 = 16; o2 > 0; o2 >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o2);
-        if (lane == 0) o[j] = __fdiv_rn(__double2float_rn(acc), (float)k);
+        const float* a = xr + j * (size_t)k;
+        for (int l0 = 0; l0 < nleaves; l0 += 4) {
+            const int l = l0 + grp;
+            float v = 0.0f;
+            int2 lf = make_int2(0, 0);
+            if (l < nleaves) {
+                lf = leaves[l];
+                if (lf.y >= 8) {
+                    const int full = lf.y - lf.y % 8;
+                    v = __ldg(a + lf.x + c);
+                    for (int i = 8; i < full; i += 8) v = __fadd_rn(v, __ldg(a + lf.x + i + c));
+                }
+            }
+            v = __fadd_rn(v, __shfl_xor_sync(0xffffffffu, v, 1));
+            v = __fadd_rn(v, __shfl_xor_sync(0xffffffffu, v, 2));
+            v = __fadd_rn(v, __shfl_xor_sync(0xffffffffu, v, 4));
+            if (l < nleaves && c == 0) {
+                int i = lf.y - lf.y % 8;
+                if (lf.y < 8) {
+                    v = -0.0f;
+                    i = 0;
+                }
+                for (; i < lf.y; ++i) v = __fadd_rn(v, __ldg(a + lf.x + i));
+                sums[l] = v;
+            }
+        }
+        __syncwarp();
+        if (lane == 0) o[j] = __fdiv_rn(pw_combine(sums, k), (float)k);
+        __syncwarp();
     }
+}
+
+// Launch shape of k_scrunch for factor k: 256 threads while the leaf table and eight
+// leaf-sum rows fit 48 KB, fewer warps above that (up to the opt-in shared-memory size).
+static int launch_scrunch(const float* x, const TrialArrays& A, int k, int ntrials,
+                          size_t max_lo, float* lores, cudaStream_t st)
+{
+    const int nleaves = pw_num_leaves(k);
+    const size_t per_warp = (size_t)nleaves * sizeof(float);
+    const size_t table = (size_t)nleaves * sizeof(int2);
+    int warps = 8;
+    while (warps > 1 && table + warps * per_warp > 48 * 1024) warps >>= 1;
+    const size_t smem = table + warps * per_warp;
+    if (smem > 200 * 1024) return set_error(RT_EINVAL, "scrunch factor too large");
+    if (smem > 48 * 1024)
+        RT_TRY_CUDA(cudaFuncSetAttribute(k_scrunch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem));
+    const unsigned threads = 32u * warps;
+    dim3 g((unsigned)std::max<size_t>(1, std::min<size_t>((max_lo + warps - 1) / warps, 4096)),
+           (unsigned)ntrials);
+    k_scrunch<<<g, threads, smem, st>>>(x, A, k, nleaves, lores);
+    return check_cuda(cudaGetLastError(), "scrunch");
 }
 
 constexpr int kStatThreads = 256;
@@ -769,7 +915,7 @@ struct SearchPlan {
     WorkItem* d_items = nullptr;
     StagePlan* d_plans = nullptr;
     float* d_scratch = nullptr;
-    int* d_counters = nullptr;          // done + slot_release + error
+    int* d_counters = nullptr;          // done + slot_release + error + finished
     unsigned long long* d_ticket = nullptr;
     float* d_ds = nullptr;
     float* d_y = nullptr;               // dereddened series
@@ -796,6 +942,11 @@ struct SearchPlan {
     // replay of the whole run as one CUDA graph (optional); the graph is keyed on the
     // run's device pointers and captured again when they change
     bool use_graph = false;
+    // bounded waits and fault injection (rt_search_set_wait_limit, rt_search_inject_fault)
+    long long spin_limit = kSpinLimit;
+    int dep_bias = 0;
+    int alloc_fail_at = 0;   // 1-based device allocation that fails; 0: none
+    int alloc_calls = 0;
     cudaGraphExec_t gexec = nullptr;
     cudaStream_t cap_stream = nullptr;
     const void* gkey[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -989,67 +1140,94 @@ static int plan_build(SearchPlan& P)
     return RT_OK;
 }
 
+template <class T>
+static void dfree(T*& p)
+{
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
 static void plan_free_device(SearchPlan& P)
 {
-    void* ptrs[] = {P.d_widths, P.d_xforms, P.d_items, P.d_plans, P.d_scratch, P.d_counters,
-                    P.d_ticket, P.d_ds, P.d_y, P.d_norm, P.d_lores, P.d_coef, P.d_rmed, P.d_part,
-                    P.d_mean, P.d_normv, P.d_len, P.d_off, P.d_lo_len, P.d_lo_off, P.d_f,
-                    P.d_useseg, P.d_dsoff};
-    for (void* p : ptrs)
-        if (p) cudaFree(p);
+    dfree(P.d_widths); dfree(P.d_xforms); dfree(P.d_items); dfree(P.d_plans);
+    dfree(P.d_scratch); dfree(P.d_counters); dfree(P.d_ticket); dfree(P.d_ds); dfree(P.d_y);
+    dfree(P.d_norm); dfree(P.d_lores); dfree(P.d_coef); dfree(P.d_rmed); dfree(P.d_part);
+    dfree(P.d_mean); dfree(P.d_normv); dfree(P.d_len); dfree(P.d_off); dfree(P.d_lo_len);
+    dfree(P.d_lo_off); dfree(P.d_f); dfree(P.d_useseg); dfree(P.d_dsoff);
     P.dev_ready = false;
 }
 
+// Device allocation of one of the plan's buffers. With an injected allocation fault
+// (rt_search_inject_fault, RT_FAULT_ALLOC) the chosen call fails as cudaMalloc would.
 template <class T>
-static int dalloc(T** p, size_t n)
+static int dalloc(SearchPlan& P, T** p, size_t n)
 {
     if (n == 0) n = 1;
+    ++P.alloc_calls;
+    if (P.alloc_fail_at > 0 && P.alloc_calls == P.alloc_fail_at)
+        return set_error(RT_ENOMEM, "device allocation %d of the plan failed (injected)",
+                         P.alloc_calls);
     RT_TRY_CUDA(cudaMalloc((void**)p, n * sizeof(T)));
     return RT_OK;
 }
 
 template <class T>
-static int upload(T** p, const std::vector<T>& v)
+static int upload(SearchPlan& P, T** p, const std::vector<T>& v)
 {
-    RT_TRY(dalloc(p, v.size()));
+    RT_TRY(dalloc(P, p, v.size()));
     if (!v.empty())
         RT_TRY_CUDA(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
     return RT_OK;
 }
 
+static int plan_alloc_device(SearchPlan& P);
+
+// Allocates and fills the plan's device buffers once. On failure every buffer allocated so
+// far is released again, so a failed call leaks nothing and can be retried.
 static int plan_prepare_device(SearchPlan& P)
 {
     if (P.dev_ready) return RT_OK;
+    P.alloc_calls = 0;
+    const int s = plan_alloc_device(P);
+    if (s != RT_OK) {
+        plan_free_device(P);
+        return s;
+    }
+    P.dev_ready = true;
+    return RT_OK;
+}
+
+static int plan_alloc_device(SearchPlan& P)
+{
     const int T = (int)P.lengths.size();
-    RT_TRY(upload(&P.d_widths, P.widths));
-    RT_TRY(upload(&P.d_items, P.items));
-    RT_TRY(upload(&P.d_plans, P.plans));
-    RT_TRY(upload(&P.d_xforms, P.xforms));
-    RT_TRY(dalloc(&P.d_scratch, (size_t)kSlots * 2 * std::max<size_t>(P.slot_floats, 1)));
-    RT_TRY(dalloc(&P.d_counters, (size_t)P.nseq * kMaxStages + kSlots + 1));
-    RT_TRY(dalloc(&P.d_ticket, 1));
+    RT_TRY(upload(P, &P.d_widths, P.widths));
+    RT_TRY(upload(P, &P.d_items, P.items));
+    RT_TRY(upload(P, &P.d_plans, P.plans));
+    RT_TRY(upload(P, &P.d_xforms, P.xforms));
+    RT_TRY(dalloc(P, &P.d_scratch, (size_t)kSlots * 2 * std::max<size_t>(P.slot_floats, 1)));
+    RT_TRY(dalloc(P, &P.d_counters, 2 * (size_t)P.nseq * kMaxStages + kSlots + 1));
+    RT_TRY(dalloc(P, &P.d_ticket, 1));
     // + 16 floats: bulk copies read whole 16-byte units around a block of rows
-    RT_TRY(dalloc(&P.d_ds, P.ds_total + 16));
+    RT_TRY(dalloc(P, &P.d_ds, P.ds_total + 16));
     if (P.cfg.deredden) {
-        RT_TRY(dalloc(&P.d_y, P.total_len));
-        RT_TRY(dalloc(&P.d_rmed, P.scrunch > 1 ? P.lo_total : P.total_len));
+        RT_TRY(dalloc(P, &P.d_y, P.total_len));
+        RT_TRY(dalloc(P, &P.d_rmed, P.scrunch > 1 ? P.lo_total : P.total_len));
         if (P.scrunch > 1) {
-            RT_TRY(dalloc(&P.d_lores, P.lo_total));
-            RT_TRY(dalloc(&P.d_coef, P.lo_total));
+            RT_TRY(dalloc(P, &P.d_lores, P.lo_total));
+            RT_TRY(dalloc(P, &P.d_coef, P.lo_total));
         }
     }
-    if (P.has_unit_factor) RT_TRY(dalloc(&P.d_norm, P.total_len));
-    RT_TRY(dalloc(&P.d_part, (size_t)T * P.stat_blocks * 3));
-    RT_TRY(dalloc(&P.d_mean, T));
-    RT_TRY(dalloc(&P.d_normv, T));
-    RT_TRY(upload(&P.d_len, P.lengths));
-    RT_TRY(upload(&P.d_off, P.offsets));
-    RT_TRY(upload(&P.d_lo_len, P.lo_len));
-    RT_TRY(upload(&P.d_lo_off, P.lo_off));
-    RT_TRY(upload(&P.d_f, P.f));
-    RT_TRY(upload(&P.d_useseg, P.use_seg));
-    RT_TRY(upload(&P.d_dsoff, P.ds_off));
-    P.dev_ready = true;
+    if (P.has_unit_factor) RT_TRY(dalloc(P, &P.d_norm, P.total_len));
+    RT_TRY(dalloc(P, &P.d_part, (size_t)T * P.stat_blocks * 3));
+    RT_TRY(dalloc(P, &P.d_mean, T));
+    RT_TRY(dalloc(P, &P.d_normv, T));
+    RT_TRY(upload(P, &P.d_len, P.lengths));
+    RT_TRY(upload(P, &P.d_off, P.offsets));
+    RT_TRY(upload(P, &P.d_lo_len, P.lo_len));
+    RT_TRY(upload(P, &P.d_lo_off, P.lo_off));
+    RT_TRY(upload(P, &P.d_f, P.f));
+    RT_TRY(upload(P, &P.d_useseg, P.use_seg));
+    RT_TRY(upload(P, &P.d_dsoff, P.ds_off));
     return RT_OK;
 }
 
@@ -1077,9 +1255,7 @@ static int plan_run(SearchPlan& P, const float* data, float* normalised_out, dou
     if (P.cfg.deredden) {
         const int k = P.scrunch;
         if (k > 1) {
-            dim3 g((unsigned)std::min<size_t>((P.max_lo * 32 + 255) / 256, 4096), (unsigned)T);
-            k_scrunch<<<g, 256, 0, st>>>(data, TA, k, P.d_lores);
-            RT_TRY_CUDA(cudaGetLastError());
+            RT_TRY(launch_scrunch(data, TA, k, T, P.max_lo, P.d_lores, st));
             RT_TRY(launch_running_median(P.d_lores, P.d_lo_len, P.d_lo_off, T, P.max_lo,
                                          (int)P.cfg.rmed_minpts, P.d_rmed, st));
             dim3 gc((unsigned)std::min<size_t>((P.max_lo + 255) / 256, 1024), (unsigned)T);
@@ -1144,7 +1320,7 @@ static int plan_run(SearchPlan& P, const float* data, float* normalised_out, dou
     }
     if (P.timing) RT_TRY_CUDA(cudaEventRecord(P.ev[2], st));
     // counters
-    const size_t ncounters = (size_t)P.nseq * kMaxStages + kSlots + 1;
+    const size_t ncounters = 2 * (size_t)P.nseq * kMaxStages + kSlots + 1;
     RT_TRY_CUDA(cudaMemsetAsync(P.d_counters, 0, ncounters * sizeof(int), st));
     RT_TRY_CUDA(cudaMemsetAsync(P.d_ticket, 0, sizeof(unsigned long long), st));
     EngineArgs A;
@@ -1165,8 +1341,11 @@ static int plan_run(SearchPlan& P, const float* data, float* normalised_out, dou
     A.done = P.d_counters;
     A.slot_release = P.d_counters + (size_t)P.nseq * kMaxStages;
     A.error = A.slot_release + kSlots;
+    A.fin = A.error + 1;
     A.ticket = P.d_ticket;
     A.phase_cycles = P.d_phase;
+    A.spin_limit = P.spin_limit;
+    A.dep_bias = P.dep_bias;
     RT_TRY_CUDA(cudaFuncSetAttribute(k_search_persistent,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)kEngineDynBytes));
@@ -1754,6 +1933,49 @@ extern "C" int rt_search_check(rt_search_plan* plan, void* stream)
     return plan_check_error(plan->p, (cudaStream_t)stream);
 }
 
+// The kernel arguments and buffers are baked into a captured graph: drop it.
+static void plan_drop_graph(SearchPlan& P)
+{
+    if (P.gexec) cudaGraphExecDestroy(P.gexec);
+    P.gexec = nullptr;
+    for (int i = 0; i < 5; ++i) P.gkey[i] = nullptr;
+}
+
+extern "C" int rt_search_set_wait_limit(rt_search_plan* plan, long long polls)
+{
+    if (!plan) return set_error(RT_EINVAL, "null argument");
+    if (polls < 1) return set_error(RT_EINVAL, "the wait limit must be at least one poll");
+    cudaDeviceSynchronize();
+    plan->p.spin_limit = polls;
+    plan_drop_graph(plan->p);
+    return RT_OK;
+}
+
+extern "C" int rt_search_inject_fault(rt_search_plan* plan, int kind, int arg)
+{
+    if (!plan) return set_error(RT_EINVAL, "null argument");
+    SearchPlan& P = plan->p;
+    cudaDeviceSynchronize();
+    switch (kind) {
+        case RT_FAULT_NONE:
+            P.dep_bias = 0;
+            P.alloc_fail_at = 0;
+            break;
+        case RT_FAULT_STAGE_WAIT:
+            P.dep_bias = 1;
+            break;
+        case RT_FAULT_ALLOC:
+            if (arg < 1) return set_error(RT_EINVAL, "the failing allocation is numbered from 1");
+            P.alloc_fail_at = arg;
+            plan_free_device(P);  // the next run allocates again
+            break;
+        default:
+            return set_error(RT_EINVAL, "unknown fault kind %d", kind);
+    }
+    plan_drop_graph(P);
+    return RT_OK;
+}
+
 extern "C" int rt_search_set_timing(rt_search_plan* plan, int enable)
 {
     if (!plan) return set_error(RT_EINVAL, "null argument");
@@ -1863,9 +2085,8 @@ extern "C" int rt_fast_running_median(const float* d_x, size_t size, size_t widt
     if (k > 1) {
         RT_TRY_CUDA(cudaMallocAsync((void**)&lores, nl * sizeof(float), st));
         RT_TRY_CUDA(cudaMallocAsync((void**)&rmed, nl * sizeof(float), st));
-        k_scrunch<<<dim3((unsigned)std::min<size_t>((nl * 32 + 255) / 256, 4096), 1), 256, 0, st>>>(
-            d_x, A, k, lores);
-        s = launch_running_median(lores, A.lo_len, A.lo_off, 1, nl, w, rmed, st);
+        s = launch_scrunch(d_x, A, k, 1, nl, lores, st);
+        if (s == RT_OK) s = launch_running_median(lores, A.lo_len, A.lo_off, 1, nl, w, rmed, st);
         if (s == RT_OK) {
             k_interp_rmed<<<dim3(std::max(1, (int)std::min<size_t>((size + 255) / 256, 4096)), 1), 256, 0, st>>>(
                 A, k, rmed, d_out);
@@ -1910,9 +2131,8 @@ extern "C" int rt_deredden(const float* d_x, size_t size, double tsamp, double w
         RT_TRY_CUDA(cudaMallocAsync((void**)&lores, nl * sizeof(float), st));
         RT_TRY_CUDA(cudaMallocAsync((void**)&rmed, nl * sizeof(float), st));
         RT_TRY_CUDA(cudaMallocAsync((void**)&coef, nl * sizeof(double2), st));
-        k_scrunch<<<dim3((unsigned)std::min<size_t>((nl * 32 + 255) / 256, 4096), 1), 256, 0, st>>>(
-            d_x, A, k, lores);
-        s = launch_running_median(lores, A.lo_len, A.lo_off, 1, nl, w, rmed, st);
+        s = launch_scrunch(d_x, A, k, 1, nl, lores, st);
+        if (s == RT_OK) s = launch_running_median(lores, A.lo_len, A.lo_off, 1, nl, w, rmed, st);
         if (s == RT_OK) {
             k_interp_coef<<<dim3((unsigned)std::min<size_t>((nl + 255) / 256, 1024), 1), 256, 0, st>>>(
                 A, k, rmed, coef);

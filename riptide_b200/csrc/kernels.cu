@@ -89,52 +89,59 @@ int fused_rollback_add(const float* x, const float* y, size_t size, size_t shift
     return check_cuda(cudaGetLastError(), "fused_rollback_add");
 }
 
-// One CTA: chunked scan in double of the first min(size, nsum) sums, then the wraps.
-__global__ void k_circular_prefix_sum(const float* __restrict__ x, size_t size, size_t nsum,
-                                      float* __restrict__ out)
+// circular_prefix_sum (kernels.hpp:73-101). The first min(size, nsum) sums are the
+// reference's: one double accumulator taking the values in order, each partial sum rounded
+// to float. That order is kept exactly (a parallel scan rounds differently whenever a partial
+// sum is not representable in double, which random data of a few hundred thousand values
+// already reaches): one CTA stages chunks of x in shared memory, thread 0 runs the sequential
+// double sum over them, and the CTA writes the rounded sums back.
+constexpr int kCpsChunk = 4096;
+
+__global__ void __launch_bounds__(256) k_cps_head(const float* __restrict__ x, size_t jmax,
+                                                  float* __restrict__ out)
 {
-    __shared__ double s_part[1024];
-    __shared__ float s_sumx;
-    const size_t jmax = size < nsum ? size : nsum;
-    const int T = blockDim.x, tid = threadIdx.x;
-    const size_t chunk = (jmax + T - 1) / T;
-    const size_t c0 = std::min(jmax, tid * chunk), c1 = std::min(jmax, c0 + chunk);
-    double local = 0.0;
-    for (size_t c = c0; c < c1; ++c) local += (double)x[c];
-    s_part[tid] = local;
-    __syncthreads();
-    if (tid == 0) {
-        double run = 0.0;
-        for (int i = 0; i < T; ++i) {
-            const double v = s_part[i];
-            s_part[i] = run;
-            run += v;
+    __shared__ float sx[kCpsChunk];
+    double acc = 0.0;  // thread 0 only
+    for (size_t c0 = 0; c0 < jmax; c0 += kCpsChunk) {
+        const int n = (int)min((size_t)kCpsChunk, jmax - c0);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) sx[i] = x[c0 + i];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int i = 0; i < n; ++i) {
+                acc = __dadd_rn(acc, (double)sx[i]);
+                sx[i] = __double2float_rn(acc);
+            }
         }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) out[c0 + i] = sx[i];
+        __syncthreads();
     }
-    __syncthreads();
-    double run = s_part[tid];
-    for (size_t c = c0; c < c1; ++c) {
-        run += (double)x[c];
-        out[c] = __double2float_rn(run);
+}
+
+// The wraps beyond the first `size` sums (kernels.hpp:85-100): out[i*size + j] =
+// out[j] + float(i) * sumx with sumx = float(total) = out[size - 1]; full wraps and the last
+// partial one use the same formula.
+__global__ void k_cps_wraps(size_t size, size_t nsum, float* __restrict__ out)
+{
+    const float sumx = out[size - 1];
+    for (size_t k = size + blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nsum;
+         k += (size_t)gridDim.x * blockDim.x) {
+        const size_t i = k / size, j = k - i * size;
+        out[k] = __fadd_rn(out[j], __fmul_rn(__ull2float_rn((unsigned long long)i), sumx));
     }
-    if (c1 == jmax && c0 < c1) s_sumx = __double2float_rn(run);
-    if (jmax == 0 && tid == 0) s_sumx = 0.f;
-    __syncthreads();
-    if (nsum <= size) return;
-    const float sumx = s_sumx;
-    const size_t q = nsum / size, r = nsum % size;
-    for (size_t i = 1; i < q; ++i)
-        for (size_t j = tid; j < size; j += T)
-            out[i * size + j] = __fadd_rn(out[j], __fmul_rn((float)i, sumx));
-    for (size_t j = tid; j < r; j += T) out[q * size + j] = __fadd_rn(out[j], __fmul_rn((float)q, sumx));
 }
 
 int circular_prefix_sum(const float* x, size_t size, size_t nsum, float* out, cudaStream_t st)
 {
     if (nsum == 0) return RT_OK;
     if (size == 0) return set_error(RT_EINVAL, "input array must not be empty");
-    k_circular_prefix_sum<<<1, 1024, 0, st>>>(x, size, nsum, out);
-    return check_cuda(cudaGetLastError(), "circular_prefix_sum");
+    k_cps_head<<<1, 256, 0, st>>>(x, std::min(size, nsum), out);
+    RT_TRY_CUDA(cudaGetLastError());
+    if (nsum > size) {
+        k_cps_wraps<<<grid_for(nsum - size, 256), 256, 0, st>>>(size, nsum, out);
+        RT_TRY_CUDA(cudaGetLastError());
+    }
+    return RT_OK;
 }
 
 // ------------------------------------------------------------------------------------

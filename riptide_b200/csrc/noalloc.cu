@@ -11,7 +11,9 @@
 //    transform keeps two copies of intermediate results when it needs several passes);
 //    larger inputs are rejected with RT_EINVAL before anything is launched;
 //  * the first call on a device looks up the array's device address (cudaGetSymbolAddress)
-//    with that device current and caches it; make that first call before any stream capture;
+//    with that device current and caches it for the life of the process; make that first
+//    call before any stream capture. cudaDeviceReset after the first call is not supported:
+//    the module is loaded again at a new address and the cached one is stale;
 //  * all calls share the array and its contents stay from the last call; the error word is
 //    cleared at the start of each call, and every scratch row a call reads was written
 //    earlier in the same call, so nothing else needs clearing; calls that overlap on the GPU

@@ -299,7 +299,7 @@ class _SearchFn(object):
         return cls._fn.apply(x, search)
 
 
-def _bench_config4(ntrials=64, steps=3, warmup=2, taps=257):
+def benchmark_training_step(ntrials=64, steps=3, warmup=2, taps=257):
     """One training step of the differentiable-search workload: a learnable `taps`-tap FIR
     front end on `ntrials` series of 2^20 samples (100 us; half carry a pulsar), the search,
     loss = mean max-S/N of the injected series - mean over the noise-only ones. Returns a
@@ -373,4 +373,4 @@ if __name__ == "__main__":
     import json
     import sys
 
-    print(json.dumps(_bench_config4(*[int(a) for a in sys.argv[1:]])))
+    print(json.dumps(benchmark_training_step(*[int(a) for a in sys.argv[1:]])))

@@ -38,15 +38,45 @@ def _pool():
     return _POOL
 
 
+_STACKED_OK = None
+
+
+def _stacked_ok():
+    """Whether the stacked LAPACK call reproduces np.polyfit on this numpy. The gufunc is
+    private to numpy (its name and signature "ddd->ddid" may change between releases), so it
+    is checked once, on a fixed problem, against np.polyfit itself; if it is missing, raises
+    or differs in any bit, every fit goes through np.polyfit."""
+    global _STACKED_OK
+    if _STACKED_OK is None:
+        ok = _ulinalg is not None
+        if ok:
+            try:
+                x = np.array([[-0.7, -0.2, 0.1, 0.4, 0.9, 1.3, 2.2], [0.0, 0.5, 1.0, 1.5, 2.0, 2.5, 3.0]])
+                y = np.array([[1.0, 2.5, 0.3, 4.0, 3.3, -1.2, 0.7], [3.0, 1.0, 4.0, 1.0, 5.0, 9.0, 2.0]])
+                c = _polyfit_lapack(x, y, 2)
+                ok = all(np.array_equal(c[k], np.polyfit(x[k], y[k], 2)) for k in range(2))
+            except Exception:
+                ok = False
+        _STACKED_OK = ok
+    return _STACKED_OK
+
+
 def _polyfit_stacked(X, Y, deg):
     """np.polyfit(X[k], Y[k], deg) for every row k of X, Y (K x M), in one stacked call of the
     LAPACK least-squares routine np.polyfit uses: the same Vandermonde matrix, column scaling,
     rcond and driver call per problem, so every coefficient is the one np.polyfit returns.
-    Large stacks are split over threads (the gufunc runs without the GIL)."""
+    Large stacks are split over threads (the gufunc runs without the GIL). Falls back to one
+    np.polyfit per row where the stacked call is unavailable (_stacked_ok)."""
     K, M = X.shape
     order = int(deg) + 1
-    if _ulinalg is None:
+    if not _stacked_ok():
         return np.array([np.polyfit(X[k], Y[k], deg) for k in range(K)]).reshape(K, order)
+    return _polyfit_lapack(X, Y, deg)
+
+
+def _polyfit_lapack(X, Y, deg):
+    K, M = X.shape
+    order = int(deg) + 1
     lhs = np.empty((K, M, order))
     tmp = lhs[:, :, ::-1]  # np.vander: powers by repeated multiplication
     tmp[:, :, 0] = 1

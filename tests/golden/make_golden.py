@@ -5,6 +5,7 @@ override with RIPTIDE_REF_ROOT):
 
     make -C oracle ref            # the reference's libcpp, built from its own sources
     python tests/golden/make_golden.py
+    python tests/golden/make_golden.py dropin    # the libcpp call trace of the glue
 
 What it runs: the reference's compiled ``libcpp`` (oracle/_ref) for the C++ kernels, and the
 reference's own Python glue (src/riptide/{search,time_series,running_medians,libffa,
@@ -57,11 +58,12 @@ def _install_stubs():
     mod("schema", Schema=_Anything, And=_Anything, Or=_Anything, Optional=_Anything)
 
 
-def import_reference():
-    """Import the reference package `riptide` from REF_ROOT with the compiled libcpp."""
+def import_reference(libcpp=None):
+    """Import the reference package `riptide` from REF_ROOT with the compiled libcpp (or the
+    given stand-in for it)."""
     from oracle import oracle as O
 
-    libcpp = O.ref_libcpp()
+    libcpp = libcpp if libcpp is not None else O.ref_libcpp()
     if libcpp is None:
         raise SystemExit("reference libcpp missing: run `make -C oracle ref` first")
     _install_stubs()
@@ -81,8 +83,78 @@ def import_reference():
     return libcpp, mods
 
 
+class _CallRecorder(types.ModuleType):
+    """Stands in for the reference's ``riptide.libcpp`` module: forwards every call to it and
+    records (name, positional arguments, outputs)."""
+
+    def __init__(self, lib):
+        super().__init__("riptide.libcpp")
+        self._lib = lib
+        self.calls = []
+
+    def __getattr__(self, name):
+        fn = getattr(self._lib, name)
+
+        def call(*args):
+            out = fn(*args)
+            self.calls.append((name, args, out if isinstance(out, tuple) else (out,)))
+            return out
+
+        return call
+
+
+def make_dropin():
+    """dropin_trace.npz: every libcpp call that the reference's own glue makes -- ffa_search
+    (search.py:11-93, with TimeSeries.deredden / normalise and fast_running_median),
+    libffa.ffa2 / boxcar_snr / downsample and TimeSeries.downsample -- on seeded inputs,
+    with its arguments and the reference libcpp's outputs, plus the glue's final outputs.
+    Replaying the calls against riptide_b200.libcpp shows that the reference's glue, with
+    riptide.libcpp bound to riptide_b200.libcpp, receives the same values."""
+    from oracle import oracle as O
+
+    rec = _CallRecorder(O.ref_libcpp())
+    _, M = import_reference(libcpp=rec)
+    rng = np.random.default_rng(424242)
+    ts_cls = M["time_series"].TimeSeries
+    finals = {}
+    cases = [(1 << 15, 1e-3, dict(period_min=0.5, period_max=5.0)),
+             (40001, 5e-4, dict(period_min=0.3, period_max=3.0, bins_min=240, bins_max=260,
+                                rmed_width=1.0, rmed_minpts=51)),
+             (1 << 14, 1e-3, dict(period_min=0.8, period_max=2.0, deredden=False))]
+    for i, (n, tsamp, kw) in enumerate(cases):
+        x = M["libffa"].generate_signal(n, 0.77 / tsamp, ducy=0.03, amplitude=18.0)
+        x = (x + rng.standard_normal(n) * 0.1 + 2.0).astype(np.float32)
+        ts, pg = M["search"].ffa_search(ts_cls(x, tsamp), **kw)
+        finals[f"final{i}_z"] = ts.data  # the periodogram is the last call's output
+    y = rng.standard_normal((150, 251)).astype(np.float32)
+    M["libffa"].ffa2(y)
+    M["libffa"].boxcar_snr(y[:40], M["ffautils"].generate_width_trials(251), stdnoise=1.5)
+    M["libffa"].downsample(rng.standard_normal(20000).astype(np.float32), 13.37)
+    ts_cls(rng.standard_normal(10000).astype(np.float32), 1e-3).downsample(7.5)
+    out = dict(finals, n=len(rec.calls))
+    for k, (name, args, outs) in enumerate(rec.calls):
+        out[f"c{k}_name"] = np.array(name)
+        out[f"c{k}_nargs"] = len(args)
+        out[f"c{k}_nout"] = len(outs)
+        for j, a in enumerate(args):
+            if isinstance(a, np.ndarray):
+                out[f"c{k}_a{j}"] = a
+                out[f"c{k}_t{j}"] = np.array("array")
+            else:
+                out[f"c{k}_a{j}"] = np.array(a)
+                out[f"c{k}_t{j}"] = np.array(type(a).__name__)
+        for j, o in enumerate(outs):
+            out[f"c{k}_o{j}"] = o
+    np.savez_compressed(os.path.join(HERE, "dropin_trace.npz"), **out)
+    print("dropin_trace.npz:", [c[0] for c in rec.calls])
+
+
 def main(sections=None):
-    """Write the fixtures of `sections` (all when None): core, fold, readers."""
+    """Write the fixtures of `sections` (all when None): core, fold, readers, workerpool,
+    dropin (the last in a process of its own: it imports the glue over a call recorder)."""
+    if sections is not None and "dropin" in sections:
+        make_dropin()
+        return
     libcpp, M = import_reference()
     if sections is None or "fold" in sections:
         make_fold(M)

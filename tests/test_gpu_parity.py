@@ -1,7 +1,10 @@
 """Parity of the CUDA path (through the C ABI) with the oracle and the reference's golden
-fixtures. Tolerances: FFA transform, running median, periods and fold bins are bit-exact;
-S/N is bit-exact when its inputs are identical; downsampling and everything downstream of it
-(the reference reorders that float sum) within rtol 1e-5 plus an absolute floor."""
+fixtures. Tolerances: FFA transform, running median, scrunch, deredden, periods and fold bins
+are bit-exact; the normalised series is within one float32 ulp (the float64 mean and standard
+deviation are summed in another order than numpy's); S/N is bit-exact when its inputs are
+identical. Downsampling and everything downstream of it (the reference's build reorders that
+float32 sum) is held to rtol 1e-5 with an absolute floor of 2e-5 S/N units for values near
+zero, where a relative bound means nothing; every peak (row and width) is the same."""
 import numpy as np
 import pytest
 
@@ -164,14 +167,21 @@ def test_fast_running_median_noscrunch(rb):
 
 
 # ------------------------------------------------------------------------------ glue
+def _within_one_ulp(a, b):
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    ulp = np.spacing(np.maximum(np.abs(a), np.abs(b)))
+    return a.shape == b.shape and bool(np.all(np.abs(a.astype(np.float64) - b) <= ulp))
+
+
 def test_normalise_deredden_golden(rb, golden):
     g = golden("glue.npz")
     ts = rb.TimeSeries(g["x"], 1e-3)
-    assert np.allclose(ts.normalise().data, g["norm"], rtol=1e-6, atol=1e-6)
-    assert np.allclose(ts.deredden(0.5, minpts=51).data, g["dered_w0.5_m51"], rtol=1e-5, atol=1e-5)
-    assert np.allclose(ts.deredden(4.0, minpts=101).data, g["dered_w4_m101"], rtol=1e-5, atol=1e-5)
-    assert np.allclose(rb.fast_running_median(g["x"], 2001, 101), g["frm_w2001_m101"],
-                       rtol=1e-5, atol=1e-5)
+    assert _within_one_ulp(ts.normalise().data, g["norm"])
+    assert np.array_equal(ts.deredden(0.5, minpts=51).data, g["dered_w0.5_m51"])
+    assert np.array_equal(ts.deredden(4.0, minpts=101).data, g["dered_w4_m101"])
+    assert np.array_equal(rb.fast_running_median(g["x"], 2001, 101), g["frm_w2001_m101"])
+    assert np.array_equal(rb.fast_running_median(g["x"], 37, 41), g["frm_w37_m41"])
     tc = rb.TimeSeries(np.full(10000, 42.42, np.float32), 1e-3)
     assert np.allclose(tc.deredden(0.5, minpts=51).data, 0.0, atol=1e-5)
 
@@ -221,10 +231,9 @@ def test_ffa_search_golden(rb, golden):
         kw = {k.split("_", 1)[1]: g[k].item() for k in g if k.startswith(f"kw{i}_")}
         ts = rb.TimeSeries(g[f"x{i}"], float(g[f"tsamp{i}"]))
         tsdr, pg = rb.ffa_search(ts, **kw)
-        assert np.allclose(tsdr.data, g[f"z{i}"], rtol=1e-5, atol=1e-5)
+        assert _within_one_ulp(tsdr.data, g[f"z{i}"])
         assert np.array_equal(pg.widths, g[f"w{i}"])
-        _check_pgram(pg.periods, pg.foldbins, pg.snrs, g[f"p{i}"], g[f"fb{i}"], g[f"s{i}"],
-                     rtol=1e-4, atol=1e-4)
+        _check_pgram(pg.periods, pg.foldbins, pg.snrs, g[f"p{i}"], g[f"fb{i}"], g[f"s{i}"])
     ts = rb.TimeSeries(g["x0"], float(g["tsamp0"]))
     tsdr, pg = rb.ffa_search(ts, period_min=0.5, period_max=5.0, deredden=False,
                              already_normalised=True)
@@ -244,7 +253,7 @@ def test_batched_equals_single(rb):
         assert np.array_equal(pg.snrs, one.snrs)
         assert np.array_equal(pg.periods, one.periods)
         z, widths, p, fb, sn = O.ffa_search(s, 5e-4, **kw)
-        _check_pgram(pg.periods, pg.foldbins, pg.snrs, p, fb, sn, rtol=1e-4, atol=1e-4)
+        _check_pgram(pg.periods, pg.foldbins, pg.snrs, p, fb, sn)
 
 
 def test_batched_full_size_trial(rb):
@@ -254,8 +263,8 @@ def test_batched_full_size_trial(rb):
     pgs, zs = rb.BatchedSearch([x.size], 64e-6, period_min=0.2, period_max=30.0).search(
         [x], return_normalised=True)
     z, widths, p, fb, sn = O.ffa_search(x, 64e-6, period_min=0.2, period_max=30.0)
-    assert np.allclose(zs[0], z, rtol=1e-5, atol=1e-5)
-    _check_pgram(pgs[0].periods, pgs[0].foldbins, pgs[0].snrs, p, fb, sn, rtol=1e-4, atol=1e-4)
+    assert _within_one_ulp(zs[0], z)
+    _check_pgram(pgs[0].periods, pgs[0].foldbins, pgs[0].snrs, p, fb, sn)
 
 
 def test_pipeline_equals_batched(rb):
@@ -327,8 +336,8 @@ def test_batched_engine_other_bins(rb, bmin, bmax, ducy, pmax):
     pgs, zs = bs.search([x], return_normalised=True)
     z, widths, p, fb, sn = O.ffa_search(x, 64e-6, **kw)
     assert np.array_equal(pgs[0].widths, widths)
-    assert np.allclose(zs[0], z, rtol=1e-5, atol=1e-5)
-    _check_pgram(pgs[0].periods, pgs[0].foldbins, pgs[0].snrs, p, fb, sn, rtol=1e-4, atol=1e-4)
+    assert _within_one_ulp(zs[0], z)
+    _check_pgram(pgs[0].periods, pgs[0].foldbins, pgs[0].snrs, p, fb, sn)
     bs.close()
 
 
@@ -389,5 +398,120 @@ def test_survey_configurations_full_size(rb, config_id):
     bs.close()
     z, widths, p, fb, sn = O.ffa_search(x, cfg["tsamp"], libcpp=O.ref_libcpp(), **kw)
     assert np.array_equal(pgs[0].widths, widths)
-    assert np.allclose(zs[0], z, rtol=1e-5, atol=1e-5)
-    _check_pgram(pgs[0].periods, pgs[0].foldbins, pgs[0].snrs, p, fb, sn, rtol=1e-4, atol=1e-4)
+    assert _within_one_ulp(zs[0], z)
+    _check_pgram(pgs[0].periods, pgs[0].foldbins, pgs[0].snrs, p, fb, sn)
+
+
+def _peak_key(pk):
+    return [(int(q[4]), int(q[5])) for q in sorted(pk, key=lambda q: (q[4], q[5]))]
+
+
+def _check_peaks(peaks, polycos, ref_peaks, ref_polycos, periods):
+    """Every peak (width index, row) identical, peak S/N within 1e-5 relative, and the
+    dynamic thresholds (each width's fitted polynomial at every trial period) within 1e-5."""
+    assert _peak_key(peaks) == _peak_key(ref_peaks)
+    a = np.array([q[6] for q in sorted(peaks, key=lambda q: (q[4], q[5]))])
+    b = np.array([q[6] for q in sorted(ref_peaks, key=lambda q: (q[4], q[5]))])
+    assert np.allclose(a, b, rtol=1e-5, atol=0)
+    logf = np.log(1.0 / np.asarray(periods))
+    assert sorted(polycos) == sorted(ref_polycos)
+    for iw in ref_polycos:
+        ta = np.polyval(np.asarray(polycos[iw], np.float64), logf)
+        tb = np.polyval(np.asarray(ref_polycos[iw], np.float64), logf)
+        assert np.allclose(ta, tb, rtol=1e-5, atol=0), iw
+
+
+def test_headline_batch_against_reference(rb):
+    """Trials of the 512-trial benchmark configuration (U[0.9, 1]*2^22 samples, 64 us, white
+    + 1/f noise, pulsars in 30%, P 0.2-30 s, bins 240-260), generated and packed exactly as
+    the benchmark does and searched in one BatchedSearch replayed as a CUDA graph. Each trial
+    is compared with the reference's own libcpp periodogram (glue restated in numpy, as the
+    reference's search.py runs it): dereddened series bit-identical, normalised series within
+    one ulp, periods and fold bins identical, S/N within rtol 1e-5, and the peaks that
+    find_peaks reports on the device identical to those of the reference's find_peaks
+    (restated) on the reference's periodogram."""
+    from riptide_b200 import synth
+
+    cfg = synth.CONFIGS[3]
+    tsamp, kw = cfg["tsamp"], dict(cfg["search"])
+    data, lengths, infos = synth.make_batch(3, 8, first_index=0)
+    bs = rb.BatchedSearch(lengths, tsamp, **kw)
+    bs.enable_graph(True)
+    periods, foldbins, snrs = bs.run(data)
+    peaks = rb.find_peaks_batched(periods, foldbins, snrs, bs.row_offsets,
+                                  [n * tsamp for n in lengths], bs.widths)
+    p_all, fb_all, s_all = (periods.cpu().numpy(), foldbins.cpu().numpy().view(np.uint32),
+                            snrs.cpu().numpy())
+    host = data.cpu().numpy()
+    bs.close()
+    npulsar = 0
+    for t, n in enumerate(lengths):
+        x = host[int(bs.sample_offsets[t]):int(bs.sample_offsets[t + 1])]
+        z, widths, p, fb, sn = O.ffa_search(x, tsamp, libcpp=O.ref_libcpp(), **kw)
+        a, b = bs.row_offsets[t], bs.row_offsets[t + 1]
+        _check_pgram(p_all[a:b], fb_all[a:b], s_all[a:b], p, fb, sn)
+        ref_peaks, ref_poly = O.find_peaks(p, fb, sn, widths, n * tsamp)
+        _check_peaks(peaks[t][0], peaks[t][1], ref_peaks, ref_poly, p)
+        npulsar += bool(infos[t]["pulsars"])
+    assert npulsar >= 1  # the sample carries injected pulsars as well as noise-only trials
+
+
+def test_error_against_fp64(rb):
+    """The error of each output against FP64 arithmetic on the same input, next to the
+    reference's own error (its libcpp, float32):
+    * S/N: FP64 periodogram (FP64 downsample, FFA and boxcar S/N) of the FP64 normalised
+      series; the GPU sums the downsampled samples in FP64 and rounds once, the reference in
+      float32;
+    * dereddened series: the FP64 running-median pipeline (FP64 scrunch mean);
+    * downsampled series: FP64 window sums."""
+    from riptide_b200 import synth
+
+    cfg = synth.CONFIGS[3]
+    tsamp, kw = cfg["tsamp"], dict(cfg["search"])
+    n = int(synth.trial_lengths(3, 1, 3)[0])
+    x, _ = synth.make_trial(3, 3, n, tsamp, "cuda")
+    x = x.cpu().numpy()
+    bs = rb.BatchedSearch([n], tsamp, **kw)
+    pgs, zs = bs.search([x], return_normalised=True)
+    bs.close()
+    y = rb.TimeSeries(x, tsamp).deredden(kw["rmed_width"], minpts=kw["rmed_minpts"]).data
+    y64 = x.astype(np.float64) - _fast_running_median_f64(x.astype(np.float64),
+                                                           int(round(kw["rmed_width"] / tsamp)),
+                                                           kw["rmed_minpts"])
+    z64 = (y.astype(np.float64) - y.mean(dtype=np.float64)) / y.std(dtype=np.float64)
+    w = O.generate_width_trials(kw["bins_min"])
+    _, _, s64 = O.C().periodogram(z64, tsamp, w, kw["period_min"], kw["period_max"],
+                                  kw["bins_min"], kw["bins_max"], f64=True)
+    R = O.ref_libcpp()
+    _, _, sref = (R.periodogram(zs[0], tsamp, w.astype(np.uint64), kw["period_min"],
+                                kw["period_max"], kw["bins_min"], kw["bins_max"]) if R is not None
+                  else O.C().periodogram(zs[0], tsamp, w, kw["period_min"], kw["period_max"],
+                                         kw["bins_min"], kw["bins_max"]))
+    scale = np.maximum(1.0, np.abs(s64))
+    err_gpu = float(np.max(np.abs(pgs[0].snrs - s64) / scale))
+    err_ref = float(np.max(np.abs(sref - s64) / scale))
+    err_dered = float(np.max(np.abs(y - y64)))
+    f = 100.37
+    d = rb.downsample(zs[0], f)
+    d64 = O.C().downsample(zs[0].astype(np.float64), f, f64=True)
+    err_ds = float(np.max(np.abs(d - d64)) / np.abs(d64).max())
+    print(f"\nerror vs FP64: S/N {err_gpu:.3g} (reference {err_ref:.3g}); dereddened "
+          f"{err_dered:.3g}; downsampled {err_ds:.3g} relative to the largest value")
+    assert err_gpu <= 1e-5 and err_gpu <= err_ref * 1.5
+    assert err_dered <= 1e-3
+    assert err_ds <= 1e-6
+
+
+def _fast_running_median_f64(x, width_samples, min_points):
+    """running_medians.py:49-85 in FP64: FP64 scrunch mean, exact median, np.interp."""
+    k = int(max(1, width_samples / float(min_points)))
+    if k == 1:
+        return O.C().running_median(x.astype(np.float32), width_samples).astype(np.float64)
+    N = (x.size // k) * k
+    lo = x[:N].reshape(-1, k).mean(axis=1)
+    half = min_points // 2
+    pad = np.concatenate([np.full(half, lo[0]), lo, np.full(half, lo[-1])])
+    win = np.lib.stride_tricks.sliding_window_view(pad, min_points)
+    rm = np.median(win, axis=1)
+    xl = np.arange(lo.size) * k + 0.5 * (k - 1)
+    return np.interp(np.arange(x.size), xl, rm)

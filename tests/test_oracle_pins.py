@@ -130,9 +130,9 @@ def test_ffafreq_formula():
 def test_glue_golden(golden):
     g = golden("glue.npz")
     x = g["x"]
-    assert np.allclose(O.normalise(x), g["norm"], rtol=1e-6, atol=1e-6)
-    assert np.allclose(O.deredden(x, 1e-3, 0.5, 51), g["dered_w0.5_m51"], rtol=1e-5, atol=1e-5)
-    assert np.allclose(O.deredden(x, 1e-3, 4.0, 101), g["dered_w4_m101"], rtol=1e-5, atol=1e-5)
+    assert np.array_equal(O.normalise(x), g["norm"])
+    assert np.array_equal(O.deredden(x, 1e-3, 0.5, 51), g["dered_w0.5_m51"])
+    assert np.array_equal(O.deredden(x, 1e-3, 4.0, 101), g["dered_w4_m101"])
     assert np.array_equal(O.fast_running_median(x, 2001, 101), g["frm_w2001_m101"])
     assert np.array_equal(O.fast_running_median(x, 37, 41), g["frm_w37_m41"])
 
@@ -143,10 +143,12 @@ def test_ffa_search_golden(golden):
         kw = {k.split("_", 1)[1]: g[k].item() for k in g if k.startswith(f"kw{i}_")}
         dered = kw.pop("deredden", True)
         z, widths, p, fb, s = O.ffa_search(g[f"x{i}"], float(g[f"tsamp{i}"]), deredden_=dered, **kw)
-        assert np.allclose(z, g[f"z{i}"], rtol=1e-5, atol=1e-5)
+        assert np.array_equal(z, g[f"z{i}"])
         assert np.array_equal(widths, g[f"w{i}"])
         assert np.array_equal(p, g[f"p{i}"]) and np.array_equal(fb, g[f"fb{i}"])
-        assert np.allclose(s, g[f"s{i}"], rtol=1e-4, atol=1e-4)
+        # the C restatement sums downsampled samples in order; the reference's build
+        # reassociates that float32 sum
+        assert np.allclose(s, g[f"s{i}"], rtol=1e-5, atol=1e-5)
         assert np.argmax(s.max(axis=1)) == np.argmax(g[f"s{i}"].max(axis=1))
 
 

@@ -13,8 +13,20 @@ from conftest import GOLDEN, load_golden
 from oracle import oracle as O
 
 # The reference's reader test data (16 samples 0..15 at 64 us, tests/data/README.md), read
-# only where the reference tree is mounted.
-REF_DATA = os.environ.get("RIPTIDE_REF_TESTDATA", "/root/reference/tests/data")
+# only where the reference tree is present: RIPTIDE_REF_TESTDATA, else the tree that
+# oracle/_ref was built from (recorded there by oracle/Makefile).
+def _ref_testdata():
+    if os.environ.get("RIPTIDE_REF_TESTDATA"):
+        return os.environ["RIPTIDE_REF_TESTDATA"]
+    rec = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle",
+                       "_ref", "source_root.txt")
+    if os.path.exists(rec):
+        with open(rec) as f:
+            return os.path.join(f.read().strip(), "tests", "data")
+    return ""
+
+
+REF_DATA = _ref_testdata()
 
 
 def _cases():
@@ -247,6 +259,25 @@ def test_stacked_polyfit_is_np_polyfit():
             C = _polyfit_stacked(X, Y, deg)
             R = np.array([np.polyfit(X[k], Y[k], deg) for k in range(X.shape[0])])
             assert np.array_equal(C, R), (M, deg)
+
+
+def test_stacked_polyfit_falls_back_when_the_private_call_differs(monkeypatch):
+    """The stacked call uses numpy's private LAPACK gufunc; it is checked against np.polyfit
+    once, and when it is missing or disagrees every fit is an np.polyfit call."""
+    from riptide_b200 import peaks
+
+    assert peaks._stacked_ok()  # numpy of this image: the stacked call is exact
+    X = np.sort(np.random.default_rng(12).uniform(-5.0, 3.0, (20, 15)), axis=1)
+    Y = np.random.default_rng(13).standard_normal((20, 15))
+    R = np.array([np.polyfit(X[k], Y[k], 2) for k in range(20)])
+    monkeypatch.setattr(peaks, "_STACKED_OK", None)
+    monkeypatch.setattr(peaks, "_ulinalg", None)
+    assert not peaks._stacked_ok()
+    assert np.array_equal(peaks._polyfit_stacked(X, Y, 2), R)
+    monkeypatch.setattr(peaks, "_STACKED_OK", None)
+    monkeypatch.setattr(peaks, "_polyfit_lapack", lambda *a: np.zeros((2, 3)))
+    assert not peaks._stacked_ok()
+    assert np.array_equal(peaks._polyfit_stacked(X, Y, 2), R)
 
 
 def test_candidate_subints_rule():
