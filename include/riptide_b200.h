@@ -173,6 +173,26 @@ int rt_search_plan_create_tuned(const uint64_t* h_lengths, size_t ntrials,
                                 const rt_search_config* cfg, const uint64_t* h_widths,
                                 size_t num_widths, const rt_search_tuning* tuning,
                                 rt_search_plan** plan);
+/* Tile choices for the transforms of a range of rows and bins, as an autotuner picks them
+ * (riptide_b200.tuning): the first rule whose ranges hold a transform's (rows, bins) sets
+ * its choices; a field left 0 keeps the plan-wide value of `tuning`.
+ *   rows_fraction  rows per job, as a fraction of what shared memory holds at these bins;
+ *   snr_threads    threads per profile in the S/N: 8 (bins <= 264 only) or 16;
+ *   max_levels     levels a job computes in shared memory (1..8, default 8): fewer levels cut
+ *                  a deep transform into more stages, whose outputs pass through L2.
+ * Results do not depend on these; only the speed does. No counterpart in the reference. */
+typedef struct rt_tile_rule {
+    uint32_t rows_min, rows_max;
+    uint32_t bins_min, bins_max;
+    double rows_fraction;
+    int snr_threads;
+    int max_levels;
+} rt_tile_rule;
+int rt_search_plan_create_rules(const uint64_t* h_lengths, size_t ntrials,
+                                const rt_search_config* cfg, const uint64_t* h_widths,
+                                size_t num_widths, const rt_search_tuning* tuning,
+                                const rt_tile_rule* rules, size_t num_rules,
+                                rt_search_plan** plan);
 /* Row offsets of each trial in the packed outputs: ntrials + 1 entries. */
 int rt_search_plan_rows(const rt_search_plan* plan, uint64_t* h_row_offsets);
 int rt_search_plan_stats(const rt_search_plan* plan, rt_search_plan_stats_t* stats);

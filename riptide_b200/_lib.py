@@ -45,6 +45,7 @@ SIGNATURES = {
     "rt_search_plan_create": (ctypes.c_int, [_u64p, _sz, _vp, _u64p, _sz, ctypes.POINTER(_vp)]),
     "rt_search_plan_rows": (ctypes.c_int, [_vp, _u64p]),
     "rt_search_plan_create_tuned": (ctypes.c_int, [_u64p, _sz, _vp, _u64p, _sz, _vp, ctypes.POINTER(_vp)]),
+    "rt_search_plan_create_rules": (ctypes.c_int, [_u64p, _sz, _vp, _u64p, _sz, _vp, _vp, _sz, ctypes.POINTER(_vp)]),
     "rt_search_plan_stats": (ctypes.c_int, [_vp, _vp]),
     "rt_search_run": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "rt_search_check": (ctypes.c_int, [_vp, _vp]),
@@ -102,6 +103,13 @@ class PlanStats(ctypes.Structure):
         "num_trials", "num_cycles", "num_transforms", "num_work_items", "num_multistage",
         "total_rows", "total_samples", "downsampled_samples", "folded_samples",
         "scrunch_factor")]
+
+
+class TileRule(ctypes.Structure):
+    _fields_ = [("rows_min", ctypes.c_uint32), ("rows_max", ctypes.c_uint32),
+                ("bins_min", ctypes.c_uint32), ("bins_max", ctypes.c_uint32),
+                ("rows_fraction", ctypes.c_double), ("snr_threads", ctypes.c_int),
+                ("max_levels", ctypes.c_int)]
 
 
 class SearchTuning(ctypes.Structure):

@@ -18,10 +18,14 @@ class BatchedSearch(object):
 
     def __init__(self, lengths, tsamp, period_min=1.0, period_max=30.0, bins_min=240,
                  bins_max=260, ducy_max=0.20, wtsp=1.5, deredden=True, rmed_width=4.0,
-                 rmed_minpts=101, already_normalised=False, widths=None, tuning=None):
+                 rmed_minpts=101, already_normalised=False, widths=None, tuning=None,
+                 rules=None):
         """`tuning`: engine tile choices, a dict with any of rows_fraction, snr_threads,
-        lag_items, rows_fraction_deep (riptide_b200.tuning.autotune picks them); results do
-        not depend on it."""
+        lag_items, rows_fraction_deep (riptide_b200.tuning.autotune picks them). `rules`:
+        per-(rows, bins) tile choices, a list of dicts with rows_min, rows_max, bins_min,
+        bins_max and any of rows_fraction, snr_threads, max_levels
+        (riptide_b200.tuning.autotune_rules picks them); the first rule holding a
+        transform's (rows, bins) applies to it. Results do not depend on either."""
         self.lengths = np.ascontiguousarray(np.asarray(lengths, dtype=np.uint64).ravel())
         self.tsamp = float(tsamp)
         self.widths = (np.asarray(widths) if widths is not None
@@ -36,7 +40,21 @@ class BatchedSearch(object):
         lp = self.lengths.ctypes.data_as(_lib._u64p)
         h = ctypes.c_void_p()
         self.tuning = dict(tuning) if tuning else None
-        if tuning:
+        self.rules = [dict(r) for r in rules] if rules else None
+        if rules:
+            tn = _lib.SearchTuning(rows_fraction=float((tuning or {}).get("rows_fraction", 0.0)),
+                                   snr_threads=int((tuning or {}).get("snr_threads", 0)),
+                                   lag_items=int((tuning or {}).get("lag_items", 0)),
+                                   rows_fraction_deep=float((tuning or {}).get("rows_fraction_deep", 0.0)))
+            arr = (_lib.TileRule * len(rules))()
+            for i, r in enumerate(rules):
+                arr[i] = _lib.TileRule(int(r["rows_min"]), int(r["rows_max"]), int(r["bins_min"]),
+                                       int(r["bins_max"]), float(r.get("rows_fraction", 0.0)),
+                                       int(r.get("snr_threads", 0)), int(r.get("max_levels", 0)))
+            _lib.check(_lib.load().rt_search_plan_create_rules(
+                lp, self.lengths.size, ctypes.byref(cfg), wp, w.size, ctypes.byref(tn), arr,
+                len(rules), ctypes.byref(h)))
+        elif tuning:
             tn = _lib.SearchTuning(rows_fraction=float(tuning.get("rows_fraction", 0.0)),
                                    snr_threads=int(tuning.get("snr_threads", 0)),
                                    lag_items=int(tuning.get("lag_items", 0)),

@@ -885,6 +885,7 @@ struct SearchPlan {
     // configuration
     rt_search_config cfg;
     rt_search_tuning tuning = {1.0, 0, 0, 0.0};
+    std::vector<rt_tile_rule> rules;    // per (rows, bins) tile choices, first match wins
     std::vector<int> widths;
     int nfast = 0;
     std::vector<size_t> lengths, offsets;
@@ -1058,15 +1059,27 @@ static int plan_build(SearchPlan& P)
                 double frac = P.tuning.rows_fraction > 0 ? std::min(1.0, P.tuning.rows_fraction) : 1.0;
                 if (rows > 8 * (size_t)cap_full && P.tuning.rows_fraction_deep > 0)
                     frac = std::min(1.0, P.tuning.rows_fraction_deep);
+                int tune_tpr = P.tuning.snr_threads, max_depth = kMaxJobDepth;
+                for (const rt_tile_rule& R : P.rules) {
+                    if (rows < R.rows_min || rows > R.rows_max || b < R.bins_min || b > R.bins_max)
+                        continue;
+                    if (R.rows_fraction > 0) frac = std::min(1.0, R.rows_fraction);
+                    if (R.snr_threads) tune_tpr = R.snr_threads;
+                    if (R.max_levels) max_depth = R.max_levels - 1;
+                    break;
+                }
                 const int capr = std::max(4, (int)((double)cap_full * frac));
                 // S/N threads per profile: 8 where the register window allows it, unless tuned
-                const int tpr = (P.tuning.snr_threads == 16) ? 16 : snr_tpr((int)b);
+                const int tpr = (tune_tpr == 16) ? 16 : snr_tpr((int)b);
                 const auto key = std::make_pair((int)rows, (long long)re * 8192 + (long long)b);
                 int pi;
                 auto itp = plan_index.find(key);
                 if (itp == plan_index.end()) {
                     StagePlan sp;
-                    if (capr < 4 || !plan_stages((int)rows, (int)re, capr, &sp))
+                    // a rule's level count that needs more stages than a plan holds falls back
+                    // to the default depth
+                    if (capr < 4 || (!plan_stages((int)rows, (int)re, capr, &sp, max_depth) &&
+                                     !plan_stages((int)rows, (int)re, capr, &sp)))
                         return set_error(RT_EINVAL, "no device plan for a %zu x %zu transform", rows, b);
                     pi = (int)P.plans.size();
                     P.plans.push_back(sp);
@@ -1712,7 +1725,8 @@ struct rt_search_plan {
 
 static int plan_create(const uint64_t* lengths, size_t ntrials, const rt_search_config* cfg,
                        const uint64_t* widths, size_t num_widths,
-                       const rt_search_tuning* tuning, rt_search_plan** out)
+                       const rt_search_tuning* tuning, rt_search_plan** out,
+                       const rt_tile_rule* rules = nullptr, size_t num_rules = 0)
 {
     if (!out || !cfg || (!lengths && ntrials) || (!widths && num_widths))
         return set_error(RT_EINVAL, "null argument");
@@ -1725,6 +1739,7 @@ static int plan_create(const uint64_t* lengths, size_t ntrials, const rt_search_
     SearchPlan& P = h->p;
     P.cfg = *cfg;
     if (tuning) P.tuning = *tuning;
+    if (rules) P.rules.assign(rules, rules + num_rules);
     for (size_t i = 0; i < num_widths; ++i) {
         // snr.hpp:21-31
         if (!(widths[i] > 0 && widths[i] < cfg->bins_min)) {
@@ -1761,10 +1776,7 @@ extern "C" int rt_search_plan_create(const uint64_t* lengths, size_t ntrials,
     return plan_create(lengths, ntrials, cfg, widths, num_widths, nullptr, out);
 }
 
-extern "C" int rt_search_plan_create_tuned(const uint64_t* lengths, size_t ntrials,
-                                           const rt_search_config* cfg, const uint64_t* widths,
-                                           size_t num_widths, const rt_search_tuning* tuning,
-                                           rt_search_plan** out)
+static int check_tuning(const rt_search_tuning* tuning)
 {
     if (tuning && !(tuning->rows_fraction >= 0.0 && tuning->rows_fraction <= 1.0))
         return set_error(RT_EINVAL, "rows_fraction must be in [0, 1]");
@@ -1773,7 +1785,39 @@ extern "C" int rt_search_plan_create_tuned(const uint64_t* lengths, size_t ntria
     if (tuning && tuning->snr_threads != 0 && tuning->snr_threads != 8 && tuning->snr_threads != 16)
         return set_error(RT_EINVAL, "snr_threads must be 0, 8 or 16");
     if (tuning && tuning->lag_items < 0) return set_error(RT_EINVAL, "lag_items must be >= 0");
+    return RT_OK;
+}
+
+extern "C" int rt_search_plan_create_tuned(const uint64_t* lengths, size_t ntrials,
+                                           const rt_search_config* cfg, const uint64_t* widths,
+                                           size_t num_widths, const rt_search_tuning* tuning,
+                                           rt_search_plan** out)
+{
+    RT_TRY(check_tuning(tuning));
     return plan_create(lengths, ntrials, cfg, widths, num_widths, tuning, out);
+}
+
+extern "C" int rt_search_plan_create_rules(const uint64_t* lengths, size_t ntrials,
+                                           const rt_search_config* cfg, const uint64_t* widths,
+                                           size_t num_widths, const rt_search_tuning* tuning,
+                                           const rt_tile_rule* rules, size_t num_rules,
+                                           rt_search_plan** plan)
+{
+    if (num_rules && !rules) return set_error(RT_EINVAL, "null argument");
+    for (size_t i = 0; i < num_rules; ++i) {
+        const rt_tile_rule& R = rules[i];
+        if (R.rows_min > R.rows_max || R.bins_min > R.bins_max)
+            return set_error(RT_EINVAL, "tile rule %zu: empty rows or bins range", i);
+        if (!(R.rows_fraction >= 0.0 && R.rows_fraction <= 1.0))
+            return set_error(RT_EINVAL, "tile rule %zu: rows_fraction must be in [0, 1]", i);
+        if (R.snr_threads != 0 && R.snr_threads != 8 && R.snr_threads != 16)
+            return set_error(RT_EINVAL, "tile rule %zu: snr_threads must be 0, 8 or 16", i);
+        if (R.max_levels < 0 || R.max_levels > kMaxJobDepth + 1)
+            return set_error(RT_EINVAL, "tile rule %zu: max_levels must be in [0, %d]", i,
+                             kMaxJobDepth + 1);
+    }
+    RT_TRY(check_tuning(tuning));
+    return plan_create(lengths, ntrials, cfg, widths, num_widths, tuning, plan, rules, num_rules);
 }
 
 extern "C" int rt_search_plan_rows(const rt_search_plan* plan, uint64_t* row_offsets)

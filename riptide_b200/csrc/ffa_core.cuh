@@ -763,7 +763,9 @@ struct StagePlan {
 // level buffers of cap_rows rows. Uses the bound: a job whose root range has R rows holds at
 // most R + 3 * 2^G rows at any level (a child range of an L-row range has <= (L + 3) / 2
 // rows, since kh, kt <= 1/2).
-bool plan_stages(int m, int rows_out, int cap_rows, StagePlan* P);
+// max_depth: the largest depth G of a job (G + 1 levels computed in shared memory); smaller
+// values cut deep transforms into more stages, whose outputs pass through L2.
+bool plan_stages(int m, int rows_out, int cap_rows, StagePlan* P, int max_depth = kMaxJobDepth);
 // Job k of stage s of a transform (host or device).
 RT_HD void node_at(int m, int d, int i, int* row0, int* rows)
 {

@@ -174,10 +174,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     run_job_levels(T, b, L.buf0, L.buf1, stride, L.ops, io);
 }
 
-bool plan_stages(int m, int rows_out, int cap_rows, StagePlan* P)
+bool plan_stages(int m, int rows_out, int cap_rows, StagePlan* P, int max_depth)
 {
     memset(P, 0, sizeof(*P));
-    if (m <= cap_rows && full_depth(m) <= kMaxJobDepth) {
+    max_depth = std::max(0, std::min(max_depth, kMaxJobDepth));
+    if (m <= cap_rows && full_depth(m) <= max_depth) {
         P->nstages = 1;
         P->D[0] = 0;
         P->R[0] = rows_out;
@@ -186,7 +187,7 @@ bool plan_stages(int m, int rows_out, int cap_rows, StagePlan* P)
         return true;
     }
     int D = 0;
-    while ((((m + (1 << D) - 1) >> D) > cap_rows) || full_depth((m + (1 << D) - 1) >> D) > kMaxJobDepth) {
+    while ((((m + (1 << D) - 1) >> D) > cap_rows) || full_depth((m + (1 << D) - 1) >> D) > max_depth) {
         ++D;
         if (D > 20) return false;
     }
@@ -199,7 +200,7 @@ bool plan_stages(int m, int rows_out, int cap_rows, StagePlan* P)
     while (D > 0) {
         if (ns >= kMaxStages) return false;
         // largest step e such that R = cap - 3 * 2^(e-1) stays >= cap / 2 (at least 1 level)
-        int e = std::min(D, kMaxJobDepth + 1);
+        int e = std::min(D, max_depth + 1);
         int R = 0;
         for (; e >= 1; --e) {
             R = cap_rows - 3 * (1 << (e - 1));

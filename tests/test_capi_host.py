@@ -113,3 +113,38 @@ def test_tuned_plan_checks_and_shapes():
                 {"rows_fraction_deep": -0.1}):
         with pytest.raises(ValueError):
             BatchedSearch([100000], 1e-3, period_min=0.5, period_max=2.0, tuning=bad)
+
+
+def test_tile_rules_checks_and_shapes():
+    # per-(rows, bins) rules change the work split of the transforms they hold only: the same
+    # periodogram rows; fewer levels per job cut the deep transforms into more stages
+    from riptide_b200 import BatchedSearch
+    from riptide_b200 import tuning as TU
+
+    kw = dict(period_min=0.2, period_max=30.0)
+    base = BatchedSearch([2 ** 22], 64e-6, **kw)
+    deep = [{"rows_min": 512, "rows_max": 4095, "bins_min": 240, "bins_max": 260, "max_levels": 5}]
+    narrow = [{"rows_min": 64, "rows_max": 127, "bins_min": 240, "bins_max": 250,
+               "rows_fraction": 0.5, "snr_threads": 16}]
+    plans = [BatchedSearch([2 ** 22], 64e-6, rules=r, **kw) for r in (deep, narrow, deep + narrow)]
+    try:
+        items = [p.stats["num_work_items"] for p in plans]
+        assert all(np.array_equal(base.row_offsets, p.row_offsets) for p in plans)
+        assert all(p.stats["num_transforms"] == base.stats["num_transforms"] for p in plans)
+        assert items[0] > base.stats["num_work_items"]           # more stages
+        assert items[1] > base.stats["num_work_items"]           # smaller jobs
+        assert items[2] == items[0] + items[1] - base.stats["num_work_items"]
+    finally:
+        base.close()
+        for p in plans:
+            p.close()
+    good = {"rows_min": 8, "rows_max": 100, "bins_min": 240, "bins_max": 260}
+    for bad in ({"rows_min": 10, "rows_max": 5}, {"bins_min": 261, "bins_max": 260},
+                {"rows_fraction": 1.5}, {"snr_threads": 12}, {"max_levels": 9}):
+        with pytest.raises(ValueError, match="tile rule"):
+            BatchedSearch([100000], 1e-3, period_min=0.5, period_max=2.0, rules=[dict(good, **bad)])
+    # the autotuner's octaves cover the search's periods, each with its rows range
+    oct_ = TU.rows_octaves([2 ** 22] * 3, 64e-6, 0.2, 30.0, 240, 260)
+    assert oct_[0]["period_max"] == 30.0 and abs(oct_[-1]["period_min"] - 0.2) < 1e-12
+    for a, b in zip(oct_, oct_[1:]):
+        assert abs(a["period_min"] - b["period_max"]) < 1e-9 and b["rows_min"] == 2 * a["rows_min"]

@@ -379,6 +379,42 @@ def test_tuned_engine_is_bit_identical(rb):
     b.close()
 
 
+def test_tile_rules_are_bit_identical(rb):
+    # per-(rows, bins) rules (rows per job, S/N threads, levels per job in shared memory)
+    # change the work split, never the periodogram; the per-octave autotuner returns rules
+    # over the octaves it timed
+    import torch
+
+    from riptide_b200 import tuning as TU
+
+    rng = np.random.default_rng(82)
+    lengths = [1 << 22, 4000000]
+    x = torch.from_numpy(np.concatenate([rng.standard_normal(n).astype(np.float32)
+                                         for n in lengths])).cuda()
+    kw = dict(period_min=0.2, period_max=30.0)
+    base = rb.BatchedSearch(lengths, 64e-6, **kw)
+    ref = [t.clone() for t in base.run(x)]
+    base.close()
+    for rules in ([{"rows_min": 512, "rows_max": 4095, "bins_min": 240, "bins_max": 260,
+                    "max_levels": 5}],
+                  [{"rows_min": 1, "rows_max": 1 << 20, "bins_min": 240, "bins_max": 249,
+                    "rows_fraction": 0.7, "snr_threads": 16},
+                   {"rows_min": 100, "rows_max": 300, "bins_min": 250, "bins_max": 260,
+                    "max_levels": 4, "rows_fraction": 0.85}]):
+        bs = rb.BatchedSearch(lengths, 64e-6, rules=rules, **kw)
+        for a, b in zip(bs.run(x), ref):
+            assert torch.equal(a, b), rules
+        bs.close()
+    res = TU.autotune_rules(lengths[:1], 64e-6, sample_trials=1, repeats=1,
+                            candidates=TU.RULE_CANDIDATES[:2], period_min=0.2, period_max=30.0)
+    assert res["rules"] and len(res["rules"]) == len(res["per_octave"])
+    assert res["ms_rules"] > 0 and res["ms_default"] > 0
+    bs = rb.BatchedSearch(lengths, 64e-6, rules=res["rules"], **kw)
+    for a, b in zip(bs.run(x), ref):
+        assert torch.equal(a, b)
+    bs.close()
+
+
 @pytest.mark.parametrize("config_id", [2, 5])
 def test_survey_configurations_full_size(rb, config_id):
     """One full-size series of the single survey-length configuration (2^23 samples, white +
