@@ -460,11 +460,14 @@ __device__ __forceinline__ void level_rows_unrolled(const RowOp* ops, int nunits
                                                     float* __restrict__ dst, int stride, int b)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int u = warp; u < nunits; u += kWarps) {
-        RowOp op = ops[u];
-        const int nr = (op.rf & kOpPair) ? 2 : 1;
-        for (int q = 0; q < nr; ++q) {
-            if (q == 1) op = second_row_op(op, b);
+    // work items are rows: item 2u is unit u's first row, 2u + 1 its second (if a pair)
+    for (int k = warp; k < 2 * nunits; k += kWarps) {
+        RowOp op = ops[k >> 1];
+        if (k & 1) {
+            if (!(op.rf & kOpPair)) continue;
+            op = second_row_op(op, b);
+        }
+        {
             float* out = dst + (size_t)(op.rf >> 3) * stride;
             const float* H = src + (size_t)op.h * sstride;
             float v[NIT];
@@ -506,30 +509,35 @@ __device__ __forceinline__ void level_rows_unrolled(const RowOp* ops, int nunits
 // column c, so a pair costs 5 shared-memory accesses per column instead of 6. Column b - 1 of
 // the second row falls to the lane whose column is b (the first column past the row in the
 // last chunk), or, when b is a multiple of 64 and no such lane exists, to column 0's lane.
+// Work items are half units (the first or the last ceil(NIT2 / 2) chunks of a unit), so the
+// ~50 units of a level spread over the warps as evenly as rows did.
 template <int NIT2>
 __device__ __forceinline__ void level_rows_pairs(const RowOp* ops, int nunits,
                                                  const float* __restrict__ src, int sstride,
                                                  float* __restrict__ dst, int stride, int b)
 {
+    constexpr int NH = (NIT2 + 1) / 2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned ub = (unsigned)b;
     const bool wrap0 = (b & 63) == 0;
-    for (int u = warp; u < nunits; u += kWarps) {
-        RowOp op = ops[u];
-        // a single row, or a pair whose tail rows differ: its rows one at a time; a pair
-        // sharing its tail row: both rows in one pass
-        const bool two = (op.rf & (kOpPair | kOpDt)) == kOpPair;
-        const int passes = ((op.rf & kOpPair) && !two) ? 2 : 1;
+    for (int k = warp; k < 2 * nunits; k += kWarps) {
+        RowOp op = ops[k >> 1];
+        const int j0 = (k & 1) * NH;
         if (op.t < 0) {  // a one-row node of level G: its source row
             float* out = dst + (size_t)(op.rf >> 3) * stride;
             const float* H = src + (size_t)op.h * sstride;
 #pragma unroll
-            for (int j = 0; j < 2 * NIT2; ++j) {
-                const int c = 32 * j + lane;
-                if (j < 2 * NIT2 - 2 || c < b) out[c] = H[c];
+            for (int jj = 0; jj < NH; ++jj) {
+                const int c = 64 * (j0 + jj) + lane;
+                if (c < b) out[c] = H[c];
+                if (c + 32 < b) out[c + 32] = H[c + 32];
             }
             continue;
         }
+        // a single row, or a pair whose tail rows differ: its rows one at a time; a pair
+        // sharing its tail row: both rows in one pass
+        const bool two = (op.rf & (kOpPair | kOpDt)) == kOpPair;
+        const int passes = ((op.rf & kOpPair) && !two) ? 2 : 1;
         for (int q = 0; q < passes; ++q) {
             if (q == 1) op = second_row_op(op, b);
             float* out = dst + (size_t)(op.rf >> 3) * stride;
@@ -537,33 +545,34 @@ __device__ __forceinline__ void level_rows_pairs(const RowOp* ops, int nunits,
             const float* H2 = H + ((op.rf & kOpDh) ? sstride : 0);
             const float* Tr = src + (size_t)op.t * sstride;
             float* out2 = out + stride;
-            // i0 = (shift + 64 j + lane) mod b from one base per row (no chain across chunks;
-            // base + 64 j < 3 b: at most two wraps), unsigned min as the conditional subtract
-            unsigned base = (unsigned)(op.shift + lane);
+            // i0 = (shift + 64 j + lane) mod b from one base per item (base + 64 j < 3 b: at
+            // most two wraps), unsigned min as the conditional subtract
+            unsigned base = (unsigned)(op.shift + lane) + 64u * j0;
+            base = min(base, base - ub);
             base = min(base, base - ub);
 #pragma unroll
-            for (int j = 0; j < NIT2; ++j) {
+            for (int jj = 0; jj < NH; ++jj) {
+                const int j = j0 + jj;
+                if (NIT2 % 2 && jj == NH - 1 && j >= NIT2) break;  // odd NIT2: shorter 2nd half
                 const int c = 64 * j + lane;
-                unsigned i0 = base + 64u * j;
+                unsigned i0 = base + 64u * jj;
                 i0 = min(i0, i0 - ub);
-                if (64 * j >= b - 32) i0 = min(i0, i0 - ub);
+                i0 = min(i0, i0 - ub);
                 unsigned i1 = i0 + 32u;
                 i1 = min(i1, i1 - ub);
-                const bool last = j == NIT2 - 1;
                 float t0 = 0.f, t1 = 0.f;
-                if (!last || c <= b) t0 = Tr[i0];
-                if (!last || c + 32 <= b) t1 = Tr[i1];
-                if (!last || c < b) out[c] = __fadd_rn(H[c], t0);
-                if (!last || c + 32 < b) out[c + 32] = __fadd_rn(H[c + 32], t1);
+                if (c <= b) t0 = Tr[i0];
+                if (c + 32 <= b) t1 = Tr[i1];
+                if (c < b) out[c] = __fadd_rn(H[c], t0);
+                if (c + 32 < b) out[c + 32] = __fadd_rn(H[c + 32], t1);
                 if (two) {
                     // second row: column c - 1 (c - 1 + 32) from the same tail values
-                    if (j == 0) {
-                        if (lane > 0) out2[c - 1] = __fadd_rn(H2[c - 1], t0);
-                        else if (wrap0) out2[b - 1] = __fadd_rn(H2[b - 1], t0);
-                    } else if (!last || c <= b) {
-                        out2[c - 1] = __fadd_rn(H2[c - 1], t0);
+                    if (c > 0) {
+                        if (c <= b) out2[c - 1] = __fadd_rn(H2[c - 1], t0);
+                    } else if (wrap0) {
+                        out2[b - 1] = __fadd_rn(H2[b - 1], t0);
                     }
-                    if (!last || c + 32 <= b) out2[c + 31] = __fadd_rn(H2[c + 31], t1);
+                    if (c + 32 <= b) out2[c + 31] = __fadd_rn(H2[c + 31], t1);
                 }
             }
         }
