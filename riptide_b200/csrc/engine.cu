@@ -72,8 +72,7 @@ struct EngineArgs {
     int nw, nfast;
     float* scratch;          // kSlots * 2 * slot_floats
     size_t slot_floats;
-    int* done;               // [nseq * kMaxStages]: jobs of the stage, once all are finished
-    int* fin;                // [nseq * kMaxStages]: jobs of the stage finished so far
+    int* done;               // [nseq * kMaxStages]
     int* slot_release;       // [kSlots]
     unsigned long long* ticket;
     int* error;              // RT_OK or an error code
@@ -155,39 +154,20 @@ __device__ __forceinline__ unsigned warps_done_acquire(const unsigned* counter)
     return v;
 }
 
-// Drops the L2 lines wholly inside [p, p + bytes) without writing them back to DRAM (their
-// contents become undefined).
-__device__ __forceinline__ void discard_l2(const void* p, size_t bytes)
-{
-    uintptr_t a = ((uintptr_t)p + 127) & ~uintptr_t(127);
-    const uintptr_t e = ((uintptr_t)p + bytes) & ~uintptr_t(127);
-    for (; a < e; a += 128) asm volatile("discard.global.L2 [%0], 128;" ::"l"(a) : "memory");
-}
-
-// Completion of an item for the other CTAs. Called by one thread after every compute warp of
-// the CTA has released the item (CTA scope); the fence makes their global writes visible at
-// GPU scope before the counters. The job that finishes its stage last (the `fin` count)
-// publishes the stage: its input, the previous stage's output in the scratch ring, is read
-// by nobody any more, so its L2 lines are dropped unwritten (otherwise every stage output
-// would be written back to DRAM when L2 evicts it, although it is consumed from L2); then
-// the stage count (`done`, which the next stage waits for) or, after the last stage, the
-// transform's scratch slot is released. The discards precede the release, so no later
-// writer of that memory can race with them.
+// Completion of an item for the other CTAs: its stage counter and, after the last job of the
+// last stage, the release of the transform's scratch slot. Called by one thread after every
+// compute warp of the CTA has released the item (CTA scope); the fence makes their global
+// writes visible at GPU scope before the counters.
 __device__ __forceinline__ void signal_item_done(const EngineArgs& A, const ItemSlot& P)
 {
     if (P.X.seq < 0 || !P.done_ok) return;
     __threadfence();
-    const size_t k = (size_t)P.X.seq * kMaxStages + P.stage;
-    const int prev = atomicAdd(A.fin + k, 1);
-    if (prev + 1 != P.jobs_of_stage) return;
-    if (P.stage > 0) {
-        const float* in = A.scratch + (size_t)(P.X.seq % kSlots) * 2 * A.slot_floats +
-                          (size_t)((P.stage - 1) & 1) * A.slot_floats;
-        discard_l2(in, (size_t)P.X.m * ffa_stride(P.X.b) * sizeof(float));
+    int* d = A.done + (size_t)P.X.seq * kMaxStages + P.stage;
+    const int prev = atomicAdd(d, 1);
+    if (P.last && prev + 1 == P.jobs_of_stage) {
         __threadfence();
+        atomicAdd(A.slot_release + (P.X.seq % kSlots), 1);
     }
-    if (P.last) atomicAdd(A.slot_release + (P.X.seq % kSlots), 1);
-    else atomicAdd(A.done + k, P.jobs_of_stage);
 }
 
 // Scheduler-side view of a claimed item: its slot contents and its dependency.
@@ -916,7 +896,7 @@ struct SearchPlan {
     WorkItem* d_items = nullptr;
     StagePlan* d_plans = nullptr;
     float* d_scratch = nullptr;
-    int* d_counters = nullptr;          // done + slot_release + error + finished
+    int* d_counters = nullptr;          // done + slot_release + error
     unsigned long long* d_ticket = nullptr;
     float* d_ds = nullptr;
     float* d_y = nullptr;               // dereddened series
@@ -1218,7 +1198,7 @@ static int plan_alloc_device(SearchPlan& P)
     RT_TRY(upload(P, &P.d_plans, P.plans));
     RT_TRY(upload(P, &P.d_xforms, P.xforms));
     RT_TRY(dalloc(P, &P.d_scratch, (size_t)kSlots * 2 * std::max<size_t>(P.slot_floats, 1)));
-    RT_TRY(dalloc(P, &P.d_counters, 2 * (size_t)P.nseq * kMaxStages + kSlots + 1));
+    RT_TRY(dalloc(P, &P.d_counters, (size_t)P.nseq * kMaxStages + kSlots + 1));
     RT_TRY(dalloc(P, &P.d_ticket, 1));
     // + 16 floats: bulk copies read whole 16-byte units around a block of rows
     RT_TRY(dalloc(P, &P.d_ds, P.ds_total + 16));
@@ -1333,7 +1313,7 @@ static int plan_run(SearchPlan& P, const float* data, float* normalised_out, dou
     }
     if (P.timing) RT_TRY_CUDA(cudaEventRecord(P.ev[2], st));
     // counters
-    const size_t ncounters = 2 * (size_t)P.nseq * kMaxStages + kSlots + 1;
+    const size_t ncounters = (size_t)P.nseq * kMaxStages + kSlots + 1;
     RT_TRY_CUDA(cudaMemsetAsync(P.d_counters, 0, ncounters * sizeof(int), st));
     RT_TRY_CUDA(cudaMemsetAsync(P.d_ticket, 0, sizeof(unsigned long long), st));
     EngineArgs A;
@@ -1354,7 +1334,6 @@ static int plan_run(SearchPlan& P, const float* data, float* normalised_out, dou
     A.done = P.d_counters;
     A.slot_release = P.d_counters + (size_t)P.nseq * kMaxStages;
     A.error = A.slot_release + kSlots;
-    A.fin = A.error + 1;
     A.ticket = P.d_ticket;
     A.phase_cycles = P.d_phase;
     A.spin_limit = P.spin_limit;

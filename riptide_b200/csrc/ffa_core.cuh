@@ -41,15 +41,13 @@ struct Node {
     int lo;     // first needed output row (node-local)
     int hi;     // one past the last needed output row
     int off;    // row of `lo` inside this level's shared buffer
-    int uoff;   // first unit (row pair or single row, see node_units) inside the level
 };
 
 struct JobTree {
     Node nodes[kMaxJobNodes];
     int level_start[kMaxJobDepth + 2];  // index of the first node of each level
     int level_rows[kMaxJobDepth + 2];   // rows stored for each level
-    int level_units[kMaxJobDepth + 2];  // units of each level
-    int op_start[kMaxJobDepth + 2];     // first unit operation of each level
+    int op_start[kMaxJobDepth + 2];     // first row operation of each level
     int depth;                          // G: nodes at this level read the global source
     int error;                          // nonzero if the job does not fit
     // Source rows of level G staged in shared memory (jobs of later stages, whose source is
@@ -77,48 +75,6 @@ RT_HD int full_depth(int rows)
     int d = 0;
     while (((rows + (1 << d) - 1) >> d) > 2) ++d;
     return d;
-}
-
-// Units. The output rows of a node with M >= 2 rows come in natural pairs that read the same
-// tail row: (2j, 2j+1) when M is even, (2j-1, 2j) when M is odd (kt = 1/2 exactly, row 0
-// alone). For every M < 16384, t(s) = int(kt*s + .5f) is equal on the two rows of a natural
-// pair (checked exhaustively with the float32 arithmetic used here), so the second row's
-// rolled tail value at column c - 1 is the first row's at column c. A unit is such a pair,
-// or a single row (a pair cut by the node's needed range [lo, hi), row 0 of an odd node,
-// the row of a one-row node). Level loops work unit by unit; a pair whose tail rows differ
-// anyway (possible only for M >= 16384) is computed as two single rows.
-RT_HD int node_units(int rows, int lo, int hi)
-{
-    if (hi <= lo) return 0;
-    if (rows < 2) return hi - lo;
-    int n = 0, a = lo;
-    if ((a & 1) != (rows & 1)) {
-        n = 1;
-        ++a;
-    }
-    return n + (hi - a + 1) / 2;
-}
-
-// First row s (node-local) of unit k of a node, and whether the unit is a pair (s, s + 1).
-RT_HD void node_unit(int rows, int lo, int hi, int k, int* s, bool* pair)
-{
-    if (rows < 2) {
-        *s = lo + k;
-        *pair = false;
-        return;
-    }
-    int a = lo;
-    if ((a & 1) != (rows & 1)) {
-        if (k == 0) {
-            *s = a;
-            *pair = false;
-            return;
-        }
-        ++a;
-        --k;
-    }
-    *s = a + 2 * k;
-    *pair = *s + 1 < hi;
 }
 
 // Builds the per-level node lists of a job (all threads of the CTA, 3 barriers).
@@ -165,7 +121,6 @@ __device__ inline void build_job_tree(JobTree& T, const JobSpec& J, int cap_rows
         nd.lo = lo;
         nd.hi = hi;
         nd.off = 0;
-        nd.uoff = 0;
         T.nodes[q] = nd;
     }
     if (tid <= G) T.level_start[tid] = (1 << tid) - 1;
@@ -174,35 +129,21 @@ __device__ inline void build_job_tree(JobTree& T, const JobSpec& J, int cap_rows
     const int warp = tid >> 5, lane = tid & 31;
     if (warp <= G) {
         const int d = warp, n = 1 << d, base = (1 << d) - 1;
-        int carry = 0, ucarry = 0;
+        int carry = 0;
         for (int b0 = 0; b0 < n; b0 += 32) {
             const int i = b0 + lane;
-            int v = 0, u = 0;
-            if (i < n) {
-                const Node nd = T.nodes[base + i];
-                v = nd.hi - nd.lo;
-                u = node_units(nd.rows, nd.lo, nd.hi);
-            }
-            int incl = v, uincl = u;
+            const int v = (i < n) ? (T.nodes[base + i].hi - T.nodes[base + i].lo) : 0;
+            int incl = v;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                const int yu = __shfl_up_sync(0xffffffffu, uincl, o);
-                if (lane >= o) {
-                    incl += y;
-                    uincl += yu;
-                }
+                if (lane >= o) incl += y;
             }
-            if (i < n) {
-                T.nodes[base + i].off = carry + incl - v;
-                T.nodes[base + i].uoff = ucarry + uincl - u;
-            }
+            if (i < n) T.nodes[base + i].off = carry + incl - v;
             carry += __shfl_sync(0xffffffffu, incl, 31);
-            ucarry += __shfl_sync(0xffffffffu, uincl, 31);
         }
         if (lane == 0) {
             T.level_rows[d] = carry;
-            T.level_units[d] = ucarry;
             if (carry > cap_rows) T.error = 2;
         }
     }
@@ -211,7 +152,7 @@ __device__ inline void build_job_tree(JobTree& T, const JobSpec& J, int cap_rows
         int acc = 0;
         for (int d = 0; d <= G; ++d) {
             T.op_start[d] = acc;
-            acc += T.level_units[d];
+            acc += T.level_rows[d];
         }
         T.op_start[G + 1] = acc;
     }
@@ -245,7 +186,6 @@ __device__ inline void build_job_tree_warp(JobTree& T, const JobSpec& J, int cap
         nd.lo = J.lo;
         nd.hi = J.hi;
         nd.off = 0;
-        nd.uoff = 0;
         T.nodes[0] = nd;
     }
     __syncwarp();
@@ -268,50 +208,34 @@ __device__ inline void build_job_tree_warp(JobTree& T, const JobSpec& J, int cap
                 nd.hi = merge_row(c.kh, p.hi - 1) + 1;
             }
             nd.off = 0;
-            nd.uoff = 0;
             T.nodes[base + i] = nd;
         }
         __syncwarp();
     }
-    // per level: exclusive prefixes of the row and unit counts -> buffer and unit offsets;
-    // then op_start
+    // per level: exclusive prefix of the row counts -> buffer offsets; then op_start
     int acc = 0;
     for (int d = 0; d <= G; ++d) {
         const int n = 1 << d, base = n - 1;
-        int carry = 0, ucarry = 0;
+        int carry = 0;
         for (int b0 = 0; b0 < n; b0 += 32) {
             const int i = b0 + lane;
-            int v = 0, u = 0;
-            if (i < n) {
-                const Node nd = T.nodes[base + i];
-                v = nd.hi - nd.lo;
-                u = node_units(nd.rows, nd.lo, nd.hi);
-            }
-            int incl = v, uincl = u;
+            const int v = (i < n) ? (T.nodes[base + i].hi - T.nodes[base + i].lo) : 0;
+            int incl = v;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                const int yu = __shfl_up_sync(0xffffffffu, uincl, o);
-                if (lane >= o) {
-                    incl += y;
-                    uincl += yu;
-                }
+                if (lane >= o) incl += y;
             }
-            if (i < n) {
-                T.nodes[base + i].off = carry + incl - v;
-                T.nodes[base + i].uoff = ucarry + uincl - u;
-            }
+            if (i < n) T.nodes[base + i].off = carry + incl - v;
             carry += __shfl_sync(0xffffffffu, incl, 31);
-            ucarry += __shfl_sync(0xffffffffu, uincl, 31);
         }
         if (lane == 0) {
             T.level_start[d] = base;
             T.level_rows[d] = carry;
-            T.level_units[d] = ucarry;
             T.op_start[d] = acc;
             if (carry > cap_rows) T.error = 2;
         }
-        acc += ucarry;
+        acc += carry;
     }
     if (lane == 0) T.op_start[G + 1] = acc;
     if (stage_source && G <= kMaxStagedDepth) {
@@ -354,14 +278,13 @@ __device__ inline void build_job_tree_warp(JobTree& T, const JobSpec& J, int cap
     __syncwarp();
 }
 
-// Index of the node holding unit u at a level (nodes sorted by `uoff`; a node without units
-// has the uoff of the next one and is never returned for a unit it does not hold).
-__device__ __forceinline__ int find_node_unit(const Node* nodes, int n, int u)
+// Index of the node holding buffer row r at a level (nodes sorted by `off`).
+__device__ __forceinline__ int find_node(const Node* nodes, int n, int r)
 {
     int lo = 0, hi = n - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (nodes[mid].uoff <= u) lo = mid;
+        if (nodes[mid].off <= r) lo = mid;
         else hi = mid - 1;
     }
     return lo;
@@ -374,73 +297,47 @@ __device__ __forceinline__ int find_node_unit(const Node* nodes, int n, int u)
 RT_HD bool halo_mode(int b) { return (b >= 225 && b <= 288) || (b >= 449 && b <= 544); }
 RT_HD int ffa_stride(int b) { return (b + 3) & ~3; }
 
-// One unit of a level: output buffer row r = h + roll(t, -shift) of the level below and, for
-// a pair, row r + 1 = (h + dh) + roll(t + dt, -(shift + 1 - dt)). For the level read from
-// global memory, h and t are global row indices; t < 0 marks a single-row node (out = row h).
-// rf = r << 3 | pair | dh << 1 | dt << 2.
-struct __align__(16) RowOp {
-    int h, t, shift, rf;
+// One output row of a level: out = row h + roll(row t, -shift) of the level below.
+// For the level read from global memory, h and t are global row indices; t < 0 marks a
+// single-row node (out = row h).
+struct RowOp {
+    int h, t, shift;
 };
-constexpr int kOpPair = 1, kOpDh = 2, kOpDt = 4;
 
-// Operation of unit u of level d.
-__device__ __forceinline__ RowOp make_unit_op(const JobTree& T, int d, int u, int b)
+// Row operation of buffer row r of level d.
+__device__ __forceinline__ RowOp make_row_op(const JobTree& T, int d, int r, int b)
 {
     const Node* lvl = T.nodes + T.level_start[d];
-    const int i = find_node_unit(lvl, 1 << d, u);
+    const int i = find_node(lvl, 1 << d, r);
     const Node nd = lvl[i];
-    int s;
-    bool pair;
-    node_unit(nd.rows, nd.lo, nd.hi, u - nd.uoff, &s, &pair);
-    const int r = nd.off + (s - nd.lo);
+    const int s = nd.lo + (r - nd.off);
     RowOp op;
     if (nd.rows == 1) {
         op.h = nd.row0;
         op.t = -1;
         op.shift = 0;
-        op.rf = r << 3;
-        return op;
-    }
-    const MergeCoef c = merge_coef(nd.rows);
-    const int h = merge_row(c.kh, s), t = merge_row(c.kt, s);
-    op.shift = (s - t) % b;
-    if (d == T.depth && T.pstaged) {
-        const int4 rg = T.src_rng[i];
-        op.h = T.src_off[i] + (nd.row0 + h - rg.x);
-        op.t = T.src_off[i] + rg.y + (nd.row0 + (nd.rows >> 1) + t - rg.z);
-    } else if (d == T.depth) {
-        op.h = nd.row0 + h;
-        op.t = nd.row0 + (nd.rows >> 1) + t;
     } else {
-        const Node* child = T.nodes + T.level_start[d + 1];
-        const Node hn = child[2 * i], tn = child[2 * i + 1];
-        op.h = hn.off + h - hn.lo;
-        op.t = tn.off + t - tn.lo;
+        const MergeCoef c = merge_coef(nd.rows);
+        const int h = merge_row(c.kh, s), t = merge_row(c.kt, s);
+        op.shift = (s - t) % b;
+        if (d == T.depth && T.pstaged) {
+            const int4 rg = T.src_rng[i];
+            op.h = T.src_off[i] + (nd.row0 + h - rg.x);
+            op.t = T.src_off[i] + rg.y + (nd.row0 + (nd.rows >> 1) + t - rg.z);
+        } else if (d == T.depth) {
+            op.h = nd.row0 + h;
+            op.t = nd.row0 + (nd.rows >> 1) + t;
+        } else {
+            const Node* child = T.nodes + T.level_start[d + 1];
+            const Node hn = child[2 * i], tn = child[2 * i + 1];
+            op.h = hn.off + h - hn.lo;
+            op.t = tn.off + t - tn.lo;
+        }
     }
-    int f = 0;
-    if (pair) {
-        // every source index above is h or t plus a constant: the second row's are +dh, +dt
-        const int dh = merge_row(c.kh, s + 1) - h, dt = merge_row(c.kt, s + 1) - t;
-        f = kOpPair | (dh ? kOpDh : 0) | (dt ? kOpDt : 0);
-    }
-    op.rf = (r << 3) | f;
     return op;
 }
 
-// Operation of the second row of a pair (as a single-row operation).
-__device__ __forceinline__ RowOp second_row_op(const RowOp& op, int b)
-{
-    RowOp o;
-    const int dt = (op.rf & kOpDt) ? 1 : 0;
-    o.h = op.h + ((op.rf & kOpDh) ? 1 : 0);
-    o.t = op.t + dt;
-    int sh = op.shift + 1 - dt;
-    o.shift = sh >= b ? sh - b : sh;
-    o.rf = (op.rf & ~7) + 8;
-    return o;
-}
-
-// Unit operations of every level of the job (one thread per unit, all levels at once).
+// Row operations of every level of the job (one thread per output row, all levels at once).
 // Call after build_job_tree; the caller synchronises before using `ops`.
 __device__ inline void build_all_ops(const JobTree& T, int b, RowOp* ops)
 {
@@ -448,187 +345,145 @@ __device__ inline void build_all_ops(const JobTree& T, int b, RowOp* ops)
     for (int g = threadIdx.x; g < total; g += kThreads) {
         int d = 0;
         while (T.op_start[d + 1] <= g) ++d;
-        ops[g] = make_unit_op(T, d, g - T.op_start[d], b);
+        ops[g] = make_row_op(T, d, g - T.op_start[d], b);
     }
 }
 
-// Computes the rows of one level, one warp per unit (1 or 2 rows, in turn), NIT = ceil(b / 32)
-// columns per lane. kGlobal: operands are rows of the global source (packed, stride b).
+// Computes the rows of one level, one warp per row, NIT = ceil(b / 32) columns per lane.
+// kGlobal: operands are rows of the global source (packed, stride b).
 template <int NIT, bool kGlobal>
-__device__ __forceinline__ void level_rows_unrolled(const RowOp* ops, int nunits,
+__device__ __forceinline__ void level_rows_unrolled(const RowOp* ops, int nrows,
                                                     const float* __restrict__ src, int sstride,
                                                     float* __restrict__ dst, int stride, int b)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // work items are rows: item 2u is unit u's first row, 2u + 1 its second (if a pair)
-    for (int k = warp; k < 2 * nunits; k += kWarps) {
-        RowOp op = ops[k >> 1];
-        if (k & 1) {
-            if (!(op.rf & kOpPair)) continue;
-            op = second_row_op(op, b);
-        }
-        {
-            float* out = dst + (size_t)(op.rf >> 3) * stride;
-            const float* H = src + (size_t)op.h * sstride;
-            float v[NIT];
-            if (op.t < 0) {
-#pragma unroll
-                for (int j = 0; j < NIT; ++j) {
-                    const int c = lane + 32 * j;
-                    if (j < NIT - 1 || c < b) v[j] = kGlobal ? __ldcg(H + c) : H[c];
-                }
-            } else {
-                const float* Tr = src + (size_t)op.t * sstride;
-                // idx = (shift + 32 j + lane) mod b, stepped by 32 (one wrap at most: b > 32)
-                int idx = op.shift + lane;
-                idx -= (idx >= b) ? b : 0;
-#pragma unroll
-                for (int j = 0; j < NIT; ++j) {
-                    const int c = lane + 32 * j;
-                    if (j < NIT - 1 || c < b)
-                        v[j] = __fadd_rn(kGlobal ? __ldcg(H + c) : H[c],
-                                         kGlobal ? __ldcg(Tr + idx) : Tr[idx]);
-                    idx += 32;
-                    idx -= (idx >= b) ? b : 0;
-                }
-            }
+    for (int r = warp; r < nrows; r += kWarps) {
+        const RowOp op = ops[r];
+        float* out = dst + (size_t)r * stride;
+        const float* H = src + (size_t)op.h * sstride;
+        float v[NIT];
+        if (op.t < 0) {
 #pragma unroll
             for (int j = 0; j < NIT; ++j) {
                 const int c = lane + 32 * j;
-                if (j < NIT - 1 || c < b) out[c] = v[j];
+                if (j < NIT - 1 || c < b) v[j] = kGlobal ? __ldcg(H + c) : H[c];
             }
+        } else {
+            // column c reads the rolled row at c + shift, or c + shift - b past the wrap
+            // (c + shift < 2 b): the test 32 j >= b - shift - lane picks the base pointer
+            const float* T0 = src + (size_t)op.t * sstride + op.shift + lane;
+            const float* T1 = T0 - b;
+            const int thr = b - op.shift - lane;
+#pragma unroll
+            for (int j = 0; j < NIT; ++j) {
+                const int c = lane + 32 * j;
+                const float* p = (32 * j >= thr) ? T1 : T0;
+                if (j < NIT - 1 || c < b)
+                    v[j] = __fadd_rn(kGlobal ? __ldcg(H + c) : H[c],
+                                     kGlobal ? __ldcg(p + 32 * j) : p[32 * j]);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < NIT; ++j) {
+            const int c = lane + 32 * j;
+            if (j < NIT - 1 || c < b) out[c] = v[j];
         }
     }
 }
 
-// Shared-memory level for the usual bins ranges. In each 64-column chunk a lane computes
-// columns c = 64 j + lane and c + 32 of the unit's first row, so every load and store of the
-// warp touches 32 consecutive words (mod b); the rolled row is read from (64 j + shift) mod
-// b on. For a pair whose rows read the same tail row, the same lane computes column c - 1 of
-// the second row: its rolled tail value, at (c - 1 + shift + 1) mod b, is the one loaded for
-// column c, so a pair costs 5 shared-memory accesses per column instead of 6. Column b - 1 of
-// the second row falls to the lane whose column is b (the first column past the row in the
-// last chunk), or, when b is a multiple of 64 and no such lane exists, to column 0's lane.
-// Work items are half units (the first or the last ceil(NIT2 / 2) chunks of a unit), so the
-// ~50 units of a level spread over the warps as evenly as rows did.
+// Shared-memory level for the usual bins ranges: in each 64-column chunk a lane computes
+// columns c = 64 j + lane and c + 32, so every load and store of the warp touches 32
+// consecutive words (mod b). Column c reads the rolled row at c + shift before the wrap and
+// at c + shift - b after it (c + shift < 2 b: one wrap at most); with c = 64 j + lane (+ 32)
+// the wrap test is 64 j (+ 32) >= b - shift - lane, an immediate compared with one register
+// per row, and picks one of two base pointers: one compare and one select per element, and
+// no dependency chain from chunk to chunk.
 template <int NIT2>
-__device__ __forceinline__ void level_rows_pairs(const RowOp* ops, int nunits,
+__device__ __forceinline__ void level_rows_pairs(const RowOp* ops, int nrows,
                                                  const float* __restrict__ src, int sstride,
                                                  float* __restrict__ dst, int stride, int b)
 {
-    constexpr int NH = (NIT2 + 1) / 2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const unsigned ub = (unsigned)b;
-    const bool wrap0 = (b & 63) == 0;
-    for (int k = warp; k < 2 * nunits; k += kWarps) {
-        RowOp op = ops[k >> 1];
-        const int j0 = (k & 1) * NH;
-        if (op.t < 0) {  // a one-row node of level G: its source row
-            float* out = dst + (size_t)(op.rf >> 3) * stride;
-            const float* H = src + (size_t)op.h * sstride;
+    for (int r = warp; r < nrows; r += kWarps) {
+        const RowOp op = ops[r];
+        float* out = dst + (size_t)r * stride + lane;
+        const float* H = src + (size_t)op.h * sstride + lane;
+        const float* T0 = src + (size_t)op.t * sstride + op.shift + lane;
+        const float* T1 = T0 - b;
+        const int thr = b - op.shift - lane;
 #pragma unroll
-            for (int jj = 0; jj < NH; ++jj) {
-                const int c = 64 * (j0 + jj) + lane;
-                if (c < b) out[c] = H[c];
-                if (c + 32 < b) out[c + 32] = H[c + 32];
-            }
-            continue;
-        }
-        // a single row, or a pair whose tail rows differ: its rows one at a time; a pair
-        // sharing its tail row: both rows in one pass
-        const bool two = (op.rf & (kOpPair | kOpDt)) == kOpPair;
-        const int passes = ((op.rf & kOpPair) && !two) ? 2 : 1;
-        for (int q = 0; q < passes; ++q) {
-            if (q == 1) op = second_row_op(op, b);
-            float* out = dst + (size_t)(op.rf >> 3) * stride;
-            const float* H = src + (size_t)op.h * sstride;
-            const float* H2 = H + ((op.rf & kOpDh) ? sstride : 0);
-            const float* Tr = src + (size_t)op.t * sstride;
-            float* out2 = out + stride;
-            // i0 = (shift + 64 j + lane) mod b from one base per item (base + 64 j < 3 b: at
-            // most two wraps), unsigned min as the conditional subtract
-            unsigned base = (unsigned)(op.shift + lane) + 64u * j0;
-            base = min(base, base - ub);
-            base = min(base, base - ub);
-#pragma unroll
-            for (int jj = 0; jj < NH; ++jj) {
-                const int j = j0 + jj;
-                if (NIT2 % 2 && jj == NH - 1 && j >= NIT2) break;  // odd NIT2: shorter 2nd half
-                const int c = 64 * j + lane;
-                unsigned i0 = base + 64u * jj;
-                i0 = min(i0, i0 - ub);
-                i0 = min(i0, i0 - ub);
-                unsigned i1 = i0 + 32u;
-                i1 = min(i1, i1 - ub);
-                float t0 = 0.f, t1 = 0.f;
-                if (c <= b) t0 = Tr[i0];
-                if (c + 32 <= b) t1 = Tr[i1];
-                if (c < b) out[c] = __fadd_rn(H[c], t0);
-                if (c + 32 < b) out[c + 32] = __fadd_rn(H[c + 32], t1);
-                if (two) {
-                    // second row: column c - 1 (c - 1 + 32) from the same tail values
-                    if (c > 0) {
-                        if (c <= b) out2[c - 1] = __fadd_rn(H2[c - 1], t0);
-                    } else if (wrap0) {
-                        out2[b - 1] = __fadd_rn(H2[b - 1], t0);
-                    }
-                    if (c + 32 <= b) out2[c + 31] = __fadd_rn(H2[c + 31], t1);
-                }
-            }
+        for (int j = 0; j < NIT2; ++j) {
+            const int c = 64 * j + lane;
+            const float* p0 = (64 * j >= thr) ? T1 : T0;
+            const float* p1 = (64 * j + 32 >= thr) ? T1 : T0;
+            if (j < NIT2 - 1 || c < b) out[64 * j] = __fadd_rn(H[64 * j], p0[64 * j]);
+            if (j < NIT2 - 1 || c + 32 < b)
+                out[64 * j + 32] = __fadd_rn(H[64 * j + 32], p1[64 * j + 32]);
         }
     }
 }
 
-// Any b: per-element wrap, no unrolling; one warp per unit, its rows in turn.
+// Any b: per-element wrap, no unrolling.
 template <bool kGlobal>
-__device__ __forceinline__ void level_rows_generic(const RowOp* ops, int nunits,
+__device__ __forceinline__ void level_rows_generic(const RowOp* ops, int nrows,
                                                    const float* __restrict__ src, int sstride,
                                                    float* __restrict__ dst, int stride, int b)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int u = warp; u < nunits; u += kWarps) {
-        RowOp op = ops[u];
-        const int nr = (op.rf & kOpPair) ? 2 : 1;
-        for (int q = 0; q < nr; ++q) {
-            if (q == 1) op = second_row_op(op, b);
-            float* out = dst + (size_t)(op.rf >> 3) * stride;
-            const float* H = src + (size_t)op.h * sstride;
-            const float* Tr = src + (size_t)(op.t < 0 ? 0 : op.t) * sstride;
-            for (int c = lane; c < b; c += 32) {
-                float v;
-                if (op.t < 0) {
-                    v = kGlobal ? __ldcg(H + c) : H[c];
-                } else {
-                    int idx = c + op.shift;
-                    idx -= (idx >= b) ? b : 0;
-                    v = kGlobal ? __fadd_rn(__ldcg(H + c), __ldcg(Tr + idx)) : __fadd_rn(H[c], Tr[idx]);
-                }
-                out[c] = v;
+    for (int r = warp; r < nrows; r += kWarps) {
+        const RowOp op = ops[r];
+        float* out = dst + (size_t)r * stride;
+        const float* H = src + (size_t)op.h * sstride;
+        const float* Tr = src + (size_t)(op.t < 0 ? 0 : op.t) * sstride;
+        for (int c = lane; c < b; c += 32) {
+            float v;
+            if (op.t < 0) {
+                v = kGlobal ? __ldcg(H + c) : H[c];
+            } else {
+                int idx = c + op.shift;
+                idx -= (idx >= b) ? b : 0;
+                v = kGlobal ? __fadd_rn(__ldcg(H + c), __ldcg(Tr + idx)) : __fadd_rn(H[c], Tr[idx]);
             }
+            out[c] = v;
         }
     }
 }
 
 template <bool kGlobal>
-__device__ __forceinline__ void level_rows(const RowOp* ops, int nunits, const float* src,
+__device__ __forceinline__ void level_rows(const RowOp* ops, int nrows, const float* src,
                                            int sstride, float* dst, int stride, int b)
 {
     if (!kGlobal && halo_mode(b)) {
         switch ((b + 63) >> 6) {
-            case 4: level_rows_pairs<4>(ops, nunits, src, sstride, dst, stride, b); return;
-            case 5: level_rows_pairs<5>(ops, nunits, src, sstride, dst, stride, b); return;
-            case 8: level_rows_pairs<8>(ops, nunits, src, sstride, dst, stride, b); return;
-            default: level_rows_pairs<9>(ops, nunits, src, sstride, dst, stride, b); return;
+            case 4: level_rows_pairs<4>(ops, nrows, src, sstride, dst, stride, b); return;
+            case 5: level_rows_pairs<5>(ops, nrows, src, sstride, dst, stride, b); return;
+            case 8: level_rows_pairs<8>(ops, nrows, src, sstride, dst, stride, b); return;
+            default: level_rows_pairs<9>(ops, nrows, src, sstride, dst, stride, b); return;
         }
     }
     const int nit = (b + 31) >> 5;
     switch (nit) {
 #define RT_NIT_CASE(N) \
-    case N: level_rows_unrolled<N, kGlobal>(ops, nunits, src, sstride, dst, stride, b); break;
+    case N: level_rows_unrolled<N, kGlobal>(ops, nrows, src, sstride, dst, stride, b); break;
         // bins 225-288 and 449-544 cover the usual searches (bins_min 240 / 480)
         RT_NIT_CASE(8) RT_NIT_CASE(9) RT_NIT_CASE(15) RT_NIT_CASE(16) RT_NIT_CASE(17)
 #undef RT_NIT_CASE
-        default: level_rows_generic<kGlobal>(ops, nunits, src, sstride, dst, stride, b);
+        default: level_rows_generic<kGlobal>(ops, nrows, src, sstride, dst, stride, b);
+    }
+}
+
+// Level computed from source rows staged in shared memory (packed, stride b): same loop as
+// the global level, plain loads.
+__device__ __forceinline__ void level_rows_staged(const RowOp* ops, int nrows, const float* src,
+                                                  float* dst, int stride, int b)
+{
+    switch ((b + 31) >> 5) {
+        case 8: level_rows_unrolled<8, false>(ops, nrows, src, b, dst, stride, b); break;
+        case 9: level_rows_unrolled<9, false>(ops, nrows, src, b, dst, stride, b); break;
+        case 15: level_rows_unrolled<15, false>(ops, nrows, src, b, dst, stride, b); break;
+        case 16: level_rows_unrolled<16, false>(ops, nrows, src, b, dst, stride, b); break;
+        case 17: level_rows_unrolled<17, false>(ops, nrows, src, b, dst, stride, b); break;
+        default: level_rows_generic<false>(ops, nrows, src, b, dst, stride, b);
     }
 }
 
@@ -669,14 +524,13 @@ __device__ inline bool run_job_levels(const JobTree& T, int b, float* buf0, floa
         // one call site per level loop kind (the loops are large once unrolled)
         const bool first = d == T.depth;
         if (first && !io.staged) {
-            level_rows<true>(lops, T.level_units[d], io.src, io.src_stride, dst, dstride, b);
+            level_rows<true>(lops, T.level_rows[d], io.src, io.src_stride, dst, dstride, b);
+        } else if (first && !io.staged_rows) {
+            level_rows_staged(lops, T.level_rows[d], io.staged, dst, dstride, b);
         } else {
-            // shared-memory source: level d + 1, or level G's source rows staged in shared
-            // memory (packed rows of b values for stage-0 jobs, the level stride for later
-            // stages)
+            // shared-memory source: level d + 1, or the staged rows of level G's children
             const float* from = first ? io.staged : ((d & 1) ? buf0 : buf1);
-            const int fstride = (first && !io.staged_rows) ? b : stride;
-            level_rows<false>(lops, T.level_units[d], from, fstride, dst, dstride, b);
+            level_rows<false>(lops, T.level_rows[d], from, stride, dst, dstride, b);
         }
         cta_sync();
     }
