@@ -607,7 +607,10 @@ static int launch_scrunch(const float* x, const TrialArrays& A, int k, int ntria
         RT_TRY_CUDA(cudaFuncSetAttribute(k_scrunch, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem));
     const unsigned threads = 32u * warps;
-    dim3 g((unsigned)std::max<size_t>(1, std::min<size_t>((max_lo + warps - 1) / warps, 4096)),
+    // every CTA builds the leaf table first, so CTAs are few and long-lived: about 8192 in
+    // all (at least 16 per series), each warp taking many points
+    const size_t per_trial = std::max<size_t>(16, 8192 / (size_t)std::max(ntrials, 1));
+    dim3 g((unsigned)std::max<size_t>(1, std::min<size_t>((max_lo + 63) / 64, per_trial)),
            (unsigned)ntrials);
     k_scrunch<<<g, threads, smem, st>>>(x, A, k, nleaves, lores);
     return check_cuda(cudaGetLastError(), "scrunch");
