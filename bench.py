@@ -160,15 +160,18 @@ def measured_peak():
 
 
 def traffic_per_trial(config_id):
-    """DRAM bytes per trial of the search kernel from the committed ncu summary of this
-    workload (captured on the batched 2^22-sample configuration only), or None."""
-    if config_id != 3:
-        return None
+    """DRAM bytes per trial of the search kernel from the committed ncu summaries (the
+    batched 2^22-sample workload and the large sweep), or None for other workloads."""
     try:
         with open(os.path.join(HERE, "profiles", "search_persistent_traffic.json")) as f:
-            return float(json.load(f)["dram_bytes_per_trial"])
+            t = json.load(f)
+        if config_id == 3:
+            return float(t["dram_bytes_per_trial"])
+        if config_id == 5:
+            return float(t["large_sweep"]["dram_bytes_per_trial"])
     except (OSError, KeyError, ValueError):
-        return None
+        pass
+    return None
 
 
 def dist_setup():
@@ -531,6 +534,7 @@ def bench_sweep(args):
     bs.close()
     peak, kind = measured_peak()
     achieved = bytes_kernel / (s2 * 1e-3) / 1e9
+    tr = traffic_per_trial(5)
     del data, outs
     torch.cuda.empty_cache()
     return {"workload": cfg["name"], "trials": args.sweep_trials, "steps": steps,
@@ -538,7 +542,8 @@ def bench_sweep(args):
             "stage_ms": {"deredden_normalise": s0, "downsample": s1, "ffa_snr": s2},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "kernel": "k_search_persistent",
-                         "peak_source": kind, "alg_bytes_per_launch": bytes_kernel}}
+                         "peak_source": kind, "alg_bytes_per_launch": bytes_kernel,
+                         "traffic": tr * args.sweep_trials if tr else None}}
 
 
 def bench_workerpool(args, cfg, data, lengths, pool):
