@@ -538,6 +538,143 @@ __device__ float pw_combine(const float* leaf_sums, int n)
     return ret;
 }
 
+// The additions of the recursion tree of n values as a program: nodes 0 .. L-1 are the leaves
+// (left to right), node L + q = node prog[q].x + node prog[q].y, in the order numpy adds
+// them (children before parents); the root is node 2L - 2 (node 0 when L = 1).
+__device__ void pw_program(int n, int2* prog)
+{
+    int fn[40], fstate[40], fleft[40];
+    int sp = 1, li = 0, q = 0, ret = 0;
+    fn[0] = n;
+    fstate[0] = 0;
+    int nleaves = 0;
+    // first pass: count leaves (node ids of internal nodes start after them)
+    {
+        int gn[40], gs[40], gp = 1;
+        gn[0] = n;
+        gs[0] = 0;
+        while (gp > 0) {
+            const int t = gp - 1, m = gn[t];
+            if (m <= kPwLeaf) {
+                ++nleaves;
+                --gp;
+                continue;
+            }
+            int m2 = m / 2;
+            m2 -= m2 % 8;
+            if (gs[t] == 0) {
+                gs[t] = 1;
+                gn[gp] = m2;
+                gs[gp++] = 0;
+            } else if (gs[t] == 1) {
+                gs[t] = 2;
+                gn[gp] = m - m2;
+                gs[gp++] = 0;
+            } else {
+                --gp;
+            }
+        }
+    }
+    while (sp > 0) {
+        const int t = sp - 1;
+        const int m = fn[t];
+        if (m <= kPwLeaf) {
+            ret = li++;
+            --sp;
+            continue;
+        }
+        int m2 = m / 2;
+        m2 -= m2 % 8;
+        if (fstate[t] == 0) {
+            fstate[t] = 1;
+            fn[sp] = m2;
+            fstate[sp++] = 0;
+        } else if (fstate[t] == 1) {
+            fleft[t] = ret;
+            fstate[t] = 2;
+            fn[sp] = m - m2;
+            fstate[sp++] = 0;
+        } else {
+            prog[q] = make_int2(fleft[t], ret);
+            ret = nleaves + q;
+            ++q;
+            --sp;
+        }
+    }
+}
+
+// Scrunch for factors whose recursion has at most 32 leaves (k up to a few thousand): a warp
+// takes 32 scrunched points at a time; its four 8-lane groups compute their leaves (one leaf
+// per group per step, one strided accumulator per lane), then every lane adds up one
+// point's leaves along the program above, so the additions of 32 points run side by side.
+// Dynamic shared memory: leaf table, program, and per warp 32 points x (2L - 1) node values.
+constexpr int kScrunchBatchLeaves = 32;
+
+__global__ void k_scrunch_batched(const float* __restrict__ x, TrialArrays A, int k, int nleaves,
+                                  float* __restrict__ lores)
+{
+    extern __shared__ __align__(16) unsigned char sm_scb[];
+    int2* leaves = reinterpret_cast<int2*>(sm_scb);
+    int2* prog = leaves + nleaves;
+    const int nn = 2 * nleaves - 1, vs = nn | 1;  // odd per-point stride: no bank conflicts
+    float* V = reinterpret_cast<float*>(prog + nleaves) + (threadIdx.x >> 5) * 32 * vs;
+    if (threadIdx.x == 0) {
+        pw_leaf_table(k, leaves);
+        pw_program(k, prog);
+    }
+    __syncthreads();
+    const int trial = blockIdx.y;
+    const size_t nl = A.lo_len[trial];
+    const float* xr = x + A.off[trial];
+    float* o = lores + A.lo_off[trial];
+    const int lane = threadIdx.x & 31;
+    const int grp = lane >> 3, c = lane & 7;
+    const size_t w0 = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
+    const size_t nwarp = ((size_t)gridDim.x * blockDim.x) >> 5;
+    for (size_t p0 = w0 * 32; p0 < nl; p0 += nwarp * 32) {
+        const int np = (int)min((size_t)32, nl - p0);
+        const int tasks = np * nleaves;
+        for (int u0 = 0; u0 < tasks; u0 += 4) {
+            const int u = u0 + grp;
+            const bool ok = u < tasks;
+            const int pt = ok ? u / nleaves : 0, l = ok ? u - pt * nleaves : 0;
+            const float* a = xr + (p0 + pt) * (size_t)k;
+            float v = 0.0f;
+            int2 lf = make_int2(0, 0);
+            if (ok) {
+                lf = leaves[l];
+                if (lf.y >= 8) {
+                    const int full = lf.y - lf.y % 8;
+                    v = __ldg(a + lf.x + c);
+                    for (int i = 8; i < full; i += 8) v = __fadd_rn(v, __ldg(a + lf.x + i + c));
+                }
+            }
+            v = __fadd_rn(v, __shfl_xor_sync(0xffffffffu, v, 1));
+            v = __fadd_rn(v, __shfl_xor_sync(0xffffffffu, v, 2));
+            v = __fadd_rn(v, __shfl_xor_sync(0xffffffffu, v, 4));
+            if (ok && c == 0) {
+                int i = lf.y - lf.y % 8;
+                if (lf.y < 8) {
+                    v = -0.0f;
+                    i = 0;
+                }
+                for (; i < lf.y; ++i) v = __fadd_rn(v, __ldg(a + lf.x + i));
+                V[pt * vs + l] = v;
+            }
+        }
+        __syncwarp();
+        if (lane < np) {
+            float* Vp = V + lane * vs;
+            for (int q = 0; q + 1 < nleaves; ++q) {
+                const int2 ab = prog[q];
+                Vp[nleaves + q] = __fadd_rn(Vp[ab.x], Vp[ab.y]);
+            }
+            o[p0 + lane] = __fdiv_rn(Vp[nn - 1], (float)k);
+        }
+        __syncwarp();
+    }
+}
+
 // lores[j] = float32 mean of x[j*k .. (j+1)*k), numpy's pairwise order (see above).
 // One warp per scrunched value; the warp's four 8-lane groups take one leaf each, a lane
 // one of the eight strided accumulators; lane 0 adds the leaf sums up the tree.
@@ -597,6 +734,19 @@ static int launch_scrunch(const float* x, const TrialArrays& A, int k, int ntria
                           size_t max_lo, float* lores, cudaStream_t st)
 {
     const int nleaves = pw_num_leaves(k);
+    if (nleaves <= kScrunchBatchLeaves) {
+        // 8 warps, each with 32 points x (2L - 1) node values
+        const size_t smem = 2 * (size_t)nleaves * sizeof(int2) +
+                            8 * 32 * (size_t)((2 * nleaves - 1) | 1) * sizeof(float);
+        const size_t per_trial = std::max<size_t>(8, 4096 / (size_t)std::max(ntrials, 1));
+        dim3 g((unsigned)std::max<size_t>(1, std::min<size_t>((max_lo + 255) / 256, per_trial)),
+               (unsigned)ntrials);
+        if (smem > 48 * 1024)
+            RT_TRY_CUDA(cudaFuncSetAttribute(k_scrunch_batched,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_scrunch_batched<<<g, 256, smem, st>>>(x, A, k, nleaves, lores);
+        return check_cuda(cudaGetLastError(), "scrunch");
+    }
     const size_t per_warp = (size_t)nleaves * sizeof(float);
     const size_t table = (size_t)nleaves * sizeof(int2);
     int warps = 8;

@@ -158,6 +158,15 @@ def test_running_median(rb, golden):
             rb.running_median(*args)
 
 
+@pytest.mark.parametrize("width,minpts", [(40000, 101), (202001, 101), (505001, 101), (1200, 7)])
+def test_fast_running_median_scrunch_orders(rb, width, minpts):
+    # scrunch factors 396, 2000, 5000, 171: the recursion of numpy's pairwise sum has 4, 16,
+    # 64 and 2 leaves (the lane-parallel kernel up to 32 leaves, the warp-per-point one above)
+    x = (np.random.default_rng(width).standard_normal(3_000_017) * 2 + 5).astype(np.float32)
+    assert np.array_equal(rb.fast_running_median(x, width, minpts),
+                          O.fast_running_median(x, width, minpts))
+
+
 def test_fast_running_median_noscrunch(rb):
     x = np.random.default_rng(5).normal(size=100)
     for w in [1, 3, 5, 7, 11, 25, 37]:
