@@ -161,19 +161,24 @@ __device__ void snr_rows_impl(const float* X, int xs, int nrows, int b, const Sn
     float* cr = C + (size_t)g * cs;
     for (int r = g; r < nrows; r += ngroups) {
         const float* xr = X + (size_t)r * xs;
-        // prefix sums (kernels.hpp:73-101): exact sums (double-float), float stores. With at
-        // most PMAX phases per thread, the thread's values are loaded once into registers.
+        // prefix sums (kernels.hpp:73-101): exact sums, float stores. The thread's segment
+        // total is summed in double (cheaper here than double-float pairs) and split into a
+        // double-float pair for the scan; the running prefix is accumulated in double-float.
+        // With at most PMAX phases per thread, the thread's values are loaded once into
+        // registers.
         constexpr bool unrolled = kUnrolled;
         float v[PMAX];
-        float lh = 0.f, ll = 0.f;
+        double seg = 0.0;
         if (unrolled) {
 #pragma unroll
             for (int j = 0; j < PMAX; ++j) v[j] = (j < i1 - i0) ? xr[i0 + j] : 0.0f;
 #pragma unroll
-            for (int j = 0; j < PMAX; ++j) df_add(lh, ll, v[j]);
+            for (int j = 0; j < PMAX; ++j) seg = __dadd_rn(seg, (double)v[j]);
         } else {
-            for (int i = i0; i < i1; ++i) df_add(lh, ll, xr[i]);
+            for (int i = i0; i < i1; ++i) seg = __dadd_rn(seg, (double)xr[i]);
         }
+        const float lh = __double2float_rn(seg);
+        const float ll = __double2float_rn(__dsub_rn(seg, (double)lh));
         float ih = lh, il = ll;  // inclusive scan over the TPR segments
 #pragma unroll
         for (int o = 1; o < TPR; o <<= 1) {
