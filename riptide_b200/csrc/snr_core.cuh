@@ -129,9 +129,21 @@ __device__ __forceinline__ void window_max(const float* cr, int start, float (&m
 #pragma unroll
     for (int j = 0; j < SB; j += 2) {
 #pragma unroll
-        for (int k = 0; k < WS::NW; ++k)
-            mx[k] = fmax3(mx[k], __fsub_rn(win[j + WS::w(k)], win[j]),
-                          __fsub_rn(win[j + 1 + WS::w(k)], win[j + 1]));
+        for (int k = 0; k < WS::NW; ++k) {
+            if (WS::w(k) % 2 == 0) {
+                // even width: both phases' differences in one packed subtraction (two
+                // round-to-nearest float32 subtractions, as __fsub_rn)
+                float d0, d1;
+                asm("{\n .reg .b64 a, b, d;\n mov.b64 a, {%2, %3};\n mov.b64 b, {%4, %5};\n"
+                    " sub.rn.f32x2 d, a, b;\n mov.b64 {%0, %1}, d;\n}"
+                    : "=f"(d0), "=f"(d1)
+                    : "f"(win[j + WS::w(k)]), "f"(win[j + 1 + WS::w(k)]), "f"(win[j]), "f"(win[j + 1]));
+                mx[k] = fmax3(mx[k], d0, d1);
+            } else {
+                mx[k] = fmax3(mx[k], __fsub_rn(win[j + WS::w(k)], win[j]),
+                              __fsub_rn(win[j + 1 + WS::w(k)], win[j + 1]));
+            }
+        }
     }
 }
 
