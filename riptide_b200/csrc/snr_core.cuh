@@ -7,12 +7,13 @@
 //     S/N = ((h + beta) * dmax - beta * C[b-1]) / stdnoise
 // (snr.hpp:49-52; the reference build fuses the first product and the subtraction, which is
 // reproduced with __fmaf_rn). Everything below follows that arithmetic exactly; the only
-// change of order is the prefix sum, done as a warp scan in double: identical to the
-// reference's sequential double sum whenever the double sums are exact (float inputs whose
-// magnitudes within one profile span less than 2^29).
+// change of order is the prefix sum: the TPR threads of a profile sum their segments (in
+// double), scan the segment totals and accumulate their running prefixes (in double-float
+// pairs), which is identical to the reference's sequential double sum whenever the sums are
+// exact (float inputs whose magnitudes within one profile span less than about 2^24).
 //
-// Work split: one warp computes C for a profile; then TPR threads share one profile, each
-// holding a window C[i .. i+SB+WMAX) in registers so that every width reads registers only.
+// Work split: TPR threads share one profile; each builds its segment of C, then holds a
+// window C[i .. i+SB+WMAX) in registers so that every width reads registers only.
 #pragma once
 #include "common.cuh"
 #include "ffa_core.cuh"
