@@ -416,9 +416,19 @@ __device__ __forceinline__ void level_rows_pairs(const RowOp* ops, int nrows,
             const int c = 64 * j + lane;
             const float* p0 = (64 * j >= thr) ? T1 : T0;
             const float* p1 = (64 * j + 32 >= thr) ? T1 : T0;
-            if (j < NIT2 - 1 || c < b) out[64 * j] = __fadd_rn(H[64 * j], p0[64 * j]);
-            if (j < NIT2 - 1 || c + 32 < b)
-                out[64 * j + 32] = __fadd_rn(H[64 * j + 32], p1[64 * j + 32]);
+            if (j < NIT2 - 1) {
+                // both columns' adds in one packed f32x2 addition
+                float s0, s1;
+                asm("{\n .reg .b64 a, b, d;\n mov.b64 a, {%2, %3};\n mov.b64 b, {%4, %5};\n"
+                    " add.rn.f32x2 d, a, b;\n mov.b64 {%0, %1}, d;\n}"
+                    : "=f"(s0), "=f"(s1)
+                    : "f"(H[64 * j]), "f"(H[64 * j + 32]), "f"(p0[64 * j]), "f"(p1[64 * j + 32]));
+                out[64 * j] = s0;
+                out[64 * j + 32] = s1;
+            } else {
+                if (c < b) out[64 * j] = __fadd_rn(H[64 * j], p0[64 * j]);
+                if (c + 32 < b) out[64 * j + 32] = __fadd_rn(H[64 * j + 32], p1[64 * j + 32]);
+            }
         }
     }
 }
