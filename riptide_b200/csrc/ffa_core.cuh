@@ -375,12 +375,29 @@ __device__ __forceinline__ void level_rows_unrolled(const RowOp* ops, int nrows,
             const float* T1 = T0 - b;
             const int thr = b - op.shift - lane;
 #pragma unroll
-            for (int j = 0; j < NIT; ++j) {
+            for (int j = 0; j < NIT; j += 2) {
                 const int c = lane + 32 * j;
                 const float* p = (32 * j >= thr) ? T1 : T0;
-                if (j < NIT - 1 || c < b)
-                    v[j] = __fadd_rn(kGlobal ? __ldcg(H + c) : H[c],
-                                     kGlobal ? __ldcg(p + 32 * j) : p[32 * j]);
+                if (j + 1 < NIT - 1) {
+                    // two columns, both inside the row: one packed f32x2 addition
+                    const float* q = (32 * j + 32 >= thr) ? T1 : T0;
+                    asm("{\n .reg .b64 a, b, d;\n mov.b64 a, {%2, %3};\n mov.b64 b, {%4, %5};\n"
+                        " add.rn.f32x2 d, a, b;\n mov.b64 {%0, %1}, d;\n}"
+                        : "=f"(v[j]), "=f"(v[j + 1])
+                        : "f"(kGlobal ? __ldcg(H + c) : H[c]), "f"(kGlobal ? __ldcg(H + c + 32) : H[c + 32]),
+                          "f"(kGlobal ? __ldcg(p + 32 * j) : p[32 * j]),
+                          "f"(kGlobal ? __ldcg(q + 32 * j + 32) : q[32 * j + 32]));
+                } else {
+                    if (j < NIT - 1 || c < b)
+                        v[j] = __fadd_rn(kGlobal ? __ldcg(H + c) : H[c],
+                                         kGlobal ? __ldcg(p + 32 * j) : p[32 * j]);
+                    if (j + 1 < NIT) {
+                        const float* q = (32 * j + 32 >= thr) ? T1 : T0;
+                        if (c + 32 < b)
+                            v[j + 1] = __fadd_rn(kGlobal ? __ldcg(H + c + 32) : H[c + 32],
+                                                 kGlobal ? __ldcg(q + 32 * j + 32) : q[32 * j + 32]);
+                    }
+                }
             }
         }
 #pragma unroll
