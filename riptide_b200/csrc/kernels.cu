@@ -326,6 +326,13 @@ int snr2(const float* x, size_t rows, size_t cols, const int* d_widths, const in
 // (acc - mean * W) / norm with W the total weight, one rounding instead of one per sample.
 // All cycles of a search are produced in the same pass, so the series is read once.
 // Factors with f + 2 > kDsHalo use k_downsample_wide instead.
+//
+// Layout of the work: a lane owns 4 consecutive staged samples of each 128-sample chunk of
+// its warp's 512, read as 16-byte vectors (realigned in registers when the segment does not
+// start on a 16-byte boundary, so the staged values and the order of the prefix sums do not
+// depend on where the series lies in memory). The prefix is a 4-sample scan in the lane and a
+// shuffle scan of the lanes' totals. Outputs of all cycles form one index range; a table gives
+// the cycle of each 32-output chunk's first index.
 // ------------------------------------------------------------------------------------
 __device__ __forceinline__ size_t first_k_at_or_after(size_t i0, double f)
 {
@@ -339,19 +346,40 @@ __device__ __forceinline__ size_t first_k_at_or_after(size_t i0, double f)
 constexpr int kDsThreads = 512;
 constexpr int kDsWarps = kDsThreads / 32;
 constexpr int kDsPerWarp = kDsStage / kDsWarps;  // staged samples per warp
-constexpr int kDsChunks = kDsPerWarp / 32;       // 32-sample chunks per warp
+constexpr int kDsQuads = kDsPerWarp / 128;       // 128-sample chunks per warp, 4 samples a lane
+constexpr int kDsTab = 1024;                     // 32-output chunks with a tabulated cycle
+static_assert(kDsPerWarp % 128 == 0, "whole chunks");
+static_assert(kDsMaxCycles <= 256, "cycle numbers are stored in bytes");
+
+// The 16-byte-aligned group A[j .. j+3] (j a multiple of 4), zero outside [lo, hi).
+__device__ __forceinline__ float4 ds_group(const float* A, int j, int lo, int hi)
+{
+    if (j >= lo && j + 4 <= hi) return __ldg(reinterpret_cast<const float4*>(A + j));
+    float4 v;
+    v.x = (j >= lo && j < hi) ? __ldg(A + j) : 0.0f;
+    v.y = (j + 1 >= lo && j + 1 < hi) ? __ldg(A + j + 1) : 0.0f;
+    v.z = (j + 2 >= lo && j + 2 < hi) ? __ldg(A + j + 2) : 0.0f;
+    v.w = (j + 3 >= lo && j + 3 < hi) ? __ldg(A + j + 3) : 0.0f;
+    return v;
+}
+
+__device__ __forceinline__ float ds_normalised(float x, double mean, double inv)
+{
+    return __double2float_rn(__ddiv_rn(__dsub_rn((double)x, mean), inv));
+}
 
 __global__ void __launch_bounds__(kDsThreads, 2)
     k_downsample_segments(DsJob job)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    double* P = reinterpret_cast<double*>(smem);                    // kDsStage + 1
-    float* zs = reinterpret_cast<float*>(P + kDsStage + 1);          // kDsStage
+    double* P = reinterpret_cast<double*>(smem);                    // kDsStage + 1 (+1 pad)
+    float* zs = reinterpret_cast<float*>(P + kDsStage + 2);          // kDsStage
     __shared__ int s_cnt[kDsMaxCycles + 1];
-    __shared__ size_t s_k0[kDsMaxCycles];
+    __shared__ long long s_kb[kDsMaxCycles];  // first output of the cycle here, minus its offset
     __shared__ double s_f[kDsMaxCycles];
     __shared__ float* s_o[kDsMaxCycles];
     __shared__ double s_part[kDsWarps];
+    __shared__ unsigned char s_tab[kDsTab];
 
     const int trial = blockIdx.y;
     const size_t N = job.lengths[trial];
@@ -365,39 +393,11 @@ __global__ void __launch_bounds__(kDsThreads, 2)
     const bool affine = job.mean != nullptr;
     float* zout = job.norm_out ? job.norm_out + job.in_off[trial] + seg0 : nullptr;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-
-    // Stage the segment + halo (and write the normalised copy if asked for). Warp w owns the
-    // staged samples [w * kDsPerWarp, (w + 1) * kDsPerWarp), lane-strided so every shared
-    // access is conflict-free.
-    // loads in batches of 8 per thread, all issued before any is used
-    double wsum = 0.0;
-    constexpr int kBatch = 8;
-    static_assert(kDsChunks % kBatch == 0, "whole batches");
-#pragma unroll
-    for (int b0 = 0; b0 < kDsChunks; b0 += kBatch) {
-        float xb[kBatch];
-#pragma unroll
-        for (int q = 0; q < kBatch; ++q) {
-            const int i = warp * kDsPerWarp + (b0 + q) * 32 + lane;
-            xb[q] = (i < L) ? __ldg(z + i) : 0.0f;
-        }
-#pragma unroll
-        for (int q = 0; q < kBatch; ++q) {
-            const int i = warp * kDsPerWarp + (b0 + q) * 32 + lane;
-            const float x = xb[q];
-            if (zout && i < L && i < seg)
-                zout[i] = __double2float_rn(__ddiv_rn(__dsub_rn((double)x, mean), inv));
-            zs[i] = x;
-            wsum += (double)x;
-        }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
-    if (lane == 0) s_part[warp] = wsum;
+    const int nc = job.ncycles;
 
     // per-cycle output ranges whose first sample imin = floor(k f) lies in the segment
     const size_t seg1 = std::min(N, seg0 + (size_t)seg);
-    if (tid < job.ncycles) {
+    if (tid < nc) {
         const int c = tid;
         const double f = job.f[c];
         const size_t n = downsampled_size(N, f);
@@ -410,19 +410,92 @@ __global__ void __launch_bounds__(kDsThreads, 2)
             cnt = k1 > k0 ? (int)(k1 - k0) : 0;
         }
         s_cnt[c] = cnt;
-        s_k0[c] = k0;
+        s_kb[c] = (long long)k0;
         s_f[c] = f;
-        s_o[c] = job.out + job.out_off[(size_t)trial * job.ncycles + c];
+        s_o[c] = job.out + job.out_off[(size_t)trial * nc + c];
     }
+
+    // Stage the segment + halo. A = z - sh is 16-byte aligned; staged sample i is A[i + sh].
+    const int sh = (int)((reinterpret_cast<uintptr_t>(z) >> 2) & 3);
+    const float* A = z - sh;
+    const int lo = sh, hi = sh + L;
+    float4 v[kDsQuads];
+    if (sh == 0) {
+#pragma unroll
+        for (int q = 0; q < kDsQuads; ++q)
+            v[q] = ds_group(A, warp * kDsPerWarp + q * 128 + 4 * lane, lo, hi);
+    } else {
+        float4 a[kDsQuads], b[kDsQuads];
+#pragma unroll
+        for (int q = 0; q < kDsQuads; ++q) {
+            const int i = warp * kDsPerWarp + q * 128 + 4 * lane;
+            a[q] = ds_group(A, i, lo, hi);
+            b[q] = ds_group(A, i + 4, lo, hi);
+        }
+#pragma unroll
+        for (int q = 0; q < kDsQuads; ++q) {
+            v[q].x = sh == 1 ? a[q].y : sh == 2 ? a[q].z : a[q].w;
+            v[q].y = sh == 1 ? a[q].z : sh == 2 ? a[q].w : b[q].x;
+            v[q].z = sh == 1 ? a[q].w : sh == 2 ? b[q].x : b[q].y;
+            v[q].w = sh == 1 ? b[q].x : sh == 2 ? b[q].y : b[q].z;
+        }
+    }
+    double wsum = 0.0;
+#pragma unroll
+    for (int q = 0; q < kDsQuads; ++q) {
+        const int i = warp * kDsPerWarp + q * 128 + 4 * lane;
+        *reinterpret_cast<float4*>(zs + i) = v[q];
+        wsum += ((double)v[q].x + (double)v[q].y) + ((double)v[q].z + (double)v[q].w);
+        if (zout) {  // the normalised copy of the segment's own samples
+            const int m = min(L, seg) - i;
+            if (m > 0) zout[i] = ds_normalised(v[q].x, mean, inv);
+            if (m > 1) zout[i + 1] = ds_normalised(v[q].y, mean, inv);
+            if (m > 2) zout[i + 2] = ds_normalised(v[q].z, mean, inv);
+            if (m > 3) zout[i + 3] = ds_normalised(v[q].w, mean, inv);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
+    if (lane == 0) s_part[warp] = wsum;
     __syncthreads();
 
-    // exclusive prefix in double: the warp's offset, then 32-sample shuffle scans
-    double carry = 0.0;
-    for (int w = 0; w < warp; ++w) carry += s_part[w];
+    if (warp == kDsWarps - 1) {
+        // output offsets of the cycles (exclusive scan of the counts) and the chunk table
+        int run = 0;
+        for (int c0 = 0; c0 < nc; c0 += 32) {
+            const int c = c0 + lane;
+            const int cnt = c < nc ? s_cnt[c] : 0;
+            int incl = cnt;
 #pragma unroll
-    for (int ch = 0; ch < kDsChunks; ++ch) {
-        const double x = (double)zs[warp * kDsPerWarp + ch * 32 + lane];
-        double incl = x;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int off = run + incl - cnt;
+            if (c < nc) {
+                s_cnt[c] = off;
+                s_kb[c] -= off;
+                for (int j = (off + 31) >> 5; j < min((int)kDsTab, (off + cnt + 31) >> 5); ++j)
+                    s_tab[j] = (unsigned char)c;
+            }
+            run += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        if (lane == 0) s_cnt[nc] = run;
+    }
+
+    // exclusive prefix in double: the preceding warps' totals, then per chunk the lane's
+    // 4-sample scan and a shuffle scan of the lanes' totals
+    double carry = lane < warp ? s_part[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) carry += __shfl_xor_sync(0xffffffffu, carry, o);
+#pragma unroll
+    for (int q = 0; q < kDsQuads; ++q) {
+        const int i = warp * kDsPerWarp + q * 128 + 4 * lane;
+        const double a0 = (double)v[q].x;
+        const double a1 = a0 + (double)v[q].y;
+        const double a2 = a1 + (double)v[q].z;
+        const double a3 = a2 + (double)v[q].w;
+        double incl = a3;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const double y = __shfl_up_sync(0xffffffffu, incl, o);
@@ -430,43 +503,40 @@ __global__ void __launch_bounds__(kDsThreads, 2)
         }
         double ex = __shfl_up_sync(0xffffffffu, incl, 1);
         if (lane == 0) ex = 0.0;
-        P[warp * kDsPerWarp + ch * 32 + lane] = carry + ex;
+        const double e = carry + ex;
+        *reinterpret_cast<double2*>(P + i) = make_double2(e, e + a0);
+        *reinterpret_cast<double2*>(P + i + 2) = make_double2(e + a1, e + a2);
         carry += __shfl_sync(0xffffffffu, incl, 31);
     }
     if (tid == kDsThreads - 1) P[kDsStage] = carry;
-    if (tid == 0) {
-        int run = 0;
-        for (int c = 0; c < job.ncycles; ++c) {
-            const int x = s_cnt[c];
-            s_cnt[c] = run;
-            run += x;
-        }
-        s_cnt[job.ncycles] = run;
-    }
     __syncthreads();
 
-    // Outputs. The outputs of all cycles form one index range [0, total), taken by the warps
-    // in chunks of 32 consecutive indices (balanced across warps). The cycle of a chunk's first
-    // index comes from ballots over the cycle offsets; a lane steps forward across the cycle
-    // boundaries inside its chunk. Sample positions are made relative to seg0: start - seg0
-    // and end - seg0 are exact (seg0 is an integer at most start), so floor, weights and
-    // clamping give the same values as the absolute FP64 bounds of downsample.hpp:58-72.
+    // Outputs, in chunks of 32 consecutive indices of the range of all cycles (balanced across
+    // warps). A lane starts from the cycle of its chunk's first index and steps forward across
+    // the cycle boundaries inside the chunk. Sample positions are made relative to seg0:
+    // start - seg0 and end - seg0 are exact (seg0 is an integer at most start), so floor,
+    // weights and clamping give the same values as the absolute FP64 bounds of
+    // downsample.hpp:58-72.
     const double seg0d = (double)seg0;
     const double lastd = (double)(N - 1 - seg0);
     const double rinv = 1.0 / inv;
-    const int nc = job.ncycles;
     const int total = s_cnt[nc];
     for (int base = warp * 32; base < total; base += kDsThreads) {
-        int c = 0;
-        for (int c0 = 1; c0 < nc; c0 += 32) {
-            const int cc = c0 + lane;
-            c += __popc(__ballot_sync(0xffffffffu, cc < nc && s_cnt[cc] <= base));
+        int c;
+        if ((base >> 5) < kDsTab) {
+            c = s_tab[base >> 5];
+        } else {
+            c = 0;
+            for (int c0 = 1; c0 < nc; c0 += 32) {
+                const int cc = c0 + lane;
+                c += __popc(__ballot_sync(0xffffffffu, cc < nc && s_cnt[cc] <= base));
+            }
         }
         const int q = base + lane;
         if (q >= total) continue;
         while (s_cnt[c + 1] <= q) ++c;
         const double f = s_f[c];
-        const size_t k = s_k0[c] + (size_t)(q - s_cnt[c]);
+        const size_t k = (size_t)(s_kb[c] + q);
         const double start = (double)k * f;
         const double end = start + f;
         const double sr = start - seg0d, er = end - seg0d;
@@ -527,6 +597,8 @@ __global__ void k_downsample_wide(DsJob job, int cycle)
 int launch_downsample(const DsJob& job_in, int ntrials, size_t max_len, cudaStream_t st)
 {
     DsJob job = job_in;
+    if (reinterpret_cast<uintptr_t>(job.in) & 3)
+        return set_error(RT_EINVAL, "the series to downsample is not 4-byte aligned");
     bool any_seg = job.norm_out != nullptr;  // the segment pass also writes the normalised copy
     double fmax = 0.0;
     for (int c = 0; c < job.ncycles; ++c) {
@@ -537,7 +609,7 @@ int launch_downsample(const DsJob& job_in, int ntrials, size_t max_len, cudaStre
     const int halo = std::min(kDsHalo, ((int)ceil(fmax) + 2 + 31) & ~31);
     job.seg = kDsStage - halo;
     if (any_seg) {
-        const size_t smem = (kDsStage + 1) * sizeof(double) + kDsStage * sizeof(float);
+        const size_t smem = (kDsStage + 2) * sizeof(double) + kDsStage * sizeof(float);
         RT_TRY_CUDA(cudaFuncSetAttribute(k_downsample_segments,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         dim3 grid((unsigned)((max_len + job.seg - 1) / job.seg), (unsigned)ntrials);
