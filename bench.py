@@ -369,6 +369,7 @@ def bench_ours(args):
     plain = bench_plain(args, cfg, data, lengths) if rank == 0 and args.plain_trials > 0 else None
     # ---- the large-sweep workload and the differentiable search (rank 0, default on) ----
     sweep = bench_sweep(args) if rank == 0 and args.sweep_trials > 0 else None
+    sweep_full = bench_sweep_full(args) if rank == 0 and args.sweep_full > 0 else None
     grad_line = None
     if rank == 0 and not args.no_grad:
         from riptide_b200.grad import benchmark_training_step
@@ -417,6 +418,7 @@ def bench_ours(args):
             "batched_vs_per_launch": (value / world / plain["per_launch"]["trials_per_s"])
             if plain and plain.get("per_launch") else None,
             "large_sweep": sweep,
+            "large_sweep_full": sweep_full,
             "grad": grad_line,
             "find_peaks": peaks_line,
             "workerpool": wp_line,
@@ -544,6 +546,63 @@ def bench_sweep(args):
                          "frac": achieved / peak, "kernel": "k_search_persistent",
                          "peak_source": kind, "alg_bytes_per_launch": bytes_kernel,
                          "traffic": tr * args.sweep_trials if tr else None}}
+
+
+def bench_sweep_full(args):
+    """The whole large batched sweep (`sweep_full` trials of 2^23 samples, P 0.2-60 s, bins
+    480-520), streamed through the GPU in batches of `sweep_trials`: each batch is generated
+    on the device, planned, searched and released before the next (all 1024 trials'
+    periodograms, 75 GB, and inputs, 32 GB, do not fit one GPU at once). Reports trials/s of
+    the searches alone (CUDA events around each batch's run) and of plan + search + release
+    (host clock, synchronised; the synthetic data generation, which stands in for data
+    arriving, is excluded), and the number of trials whose brightest periodogram row holds
+    an injected pulsar's period within 1%."""
+    import time
+
+    import torch
+
+    import riptide_b200 as rb
+    from riptide_b200 import _lib, synth
+
+    cfg = synth.CONFIGS[5]
+    chunk = max(1, args.sweep_trials or 64)
+    total, search_ms, wall_s, hits, injected = 0, 0.0, 0.0, 0, 0
+    while total < args.sweep_full:
+        n = min(chunk, args.sweep_full - total)
+        data, lengths, infos = synth.make_batch(5, n, first_index=total)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        bs = rb.BatchedSearch(lengths, cfg["tsamp"], **cfg["search"])
+        outs = bs.allocate_outputs()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        bs.run(data, outs, check=False)
+        e1.record()
+        _lib.check(_lib.load().rt_search_check(bs._plan, rb.libcpp._stream()))
+        rows = bs.row_offsets
+        best = outs[2].amax(dim=1)
+        idx = [int(torch.argmax(best[int(rows[t]):int(rows[t + 1])])) + int(rows[t])
+               for t in range(n)]
+        periods = outs[0][idx].cpu().numpy()
+        torch.cuda.synchronize()
+        search_ms += e0.elapsed_time(e1)
+        bs.close()
+        del outs
+        wall_s += time.perf_counter() - t0
+        for t, info in enumerate(infos):
+            pulsars = info.get("pulsars") or []
+            if pulsars:
+                injected += 1
+                if any(abs(periods[t] / p["period"] - 1.0) < 0.01 for p in pulsars):
+                    hits += 1
+        del data
+        torch.cuda.empty_cache()
+        total += n
+    return {"workload": cfg["name"], "trials": total, "batch_trials": chunk,
+            "batches": (total + chunk - 1) // chunk,
+            "value": total / (search_ms * 1e-3), "unit": "trials/s",
+            "search_ms": search_ms, "wall_trials_per_s": total / wall_s,
+            "trials_with_pulsar": injected, "pulsar_period_at_brightest_row": hits}
 
 
 def bench_workerpool(args, cfg, data, lengths, pool):
@@ -712,6 +771,9 @@ def main():
                     help="trials timed one at a time through the fused engine")
     ap.add_argument("--sweep-trials", type=int, default=64,
                     help="trials of the large-sweep workload timed beside the main line (0: skip)")
+    ap.add_argument("--sweep-full", type=int, default=0,
+                    help="also stream this many large-sweep trials through the GPU in batches "
+                         "of --sweep-trials (1024: the whole sweep)")
     ap.add_argument("--no-grad", action="store_true",
                     help="skip the differentiable-search training step")
     ap.add_argument("--e2e-steps", type=int, default=2)
