@@ -143,6 +143,30 @@ def test_downsample_wide_and_errors(rb):
             rb.downsample(x, f)
 
 
+def test_downsample_independent_of_alignment(rb):
+    # a device view starting 1-3 floats past a 16-byte boundary takes the kernel's realigned
+    # staging path; its outputs equal those of an aligned copy of the same samples
+    import torch
+
+    x = np.random.default_rng(12).standard_normal(300_007).astype(np.float32)
+    xt = torch.from_numpy(x).cuda()
+    for f in [1.5, 13.02, 100.37, 1953.1, 4000.0]:
+        for k in range(4):
+            view = xt[k:]
+            assert view.data_ptr() % 16 == (xt.data_ptr() + 4 * k) % 16
+            got = rb.libcpp.downsample(view, f).cpu().numpy()
+            assert np.array_equal(got, rb.libcpp.downsample(x[k:].copy(), f)), (f, k)
+            y64 = O.C().downsample(x[k:].astype(np.float64), f, f64=True)
+            assert np.max(np.abs(got - y64)) <= 1e-6 * max(1.0, np.abs(y64).max()), (f, k)
+    # a series that is not 4-byte aligned is refused before any launch
+    out = torch.empty(1000, dtype=torch.float32, device="cuda")
+    lib = rb._lib.load()
+    st = rb.libcpp._stream()
+    assert lib.rt_downsample(xt.data_ptr() + 2, 1000, 7.5, out.data_ptr(), st) == rb._lib.RT_EINVAL
+    assert "aligned" in lib.rt_last_error().decode()
+    assert lib.rt_downsample(xt.data_ptr() + 4, 1000, 7.5, out.data_ptr(), st) == rb._lib.RT_OK
+
+
 # ------------------------------------------------------------------------------ running median
 def test_running_median(rb, golden):
     g = golden("running_median.npz")
