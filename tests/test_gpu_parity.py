@@ -158,6 +158,15 @@ def test_downsample_independent_of_alignment(rb):
             assert np.array_equal(got, rb.libcpp.downsample(x[k:].copy(), f)), (f, k)
             y64 = O.C().downsample(x[k:].astype(np.float64), f, f64=True)
             assert np.max(np.abs(got - y64)) <= 1e-6 * max(1.0, np.abs(y64).max()), (f, k)
+    # a long series: several hundred segments, more CTAs than the SMs hold at once
+    x = np.random.default_rng(13).standard_normal(3_000_017).astype(np.float32)
+    xt = torch.from_numpy(x).cuda()
+    for f in [2.5, 1953.1]:
+        for k in (0, 3):
+            got = rb.libcpp.downsample(xt[k:], f).cpu().numpy()
+            assert np.array_equal(got, rb.libcpp.downsample(x[k:].copy(), f)), (f, k)
+            y64 = O.C().downsample(x[k:].astype(np.float64), f, f64=True)
+            assert np.max(np.abs(got - y64)) <= 1e-6 * max(1.0, np.abs(y64).max()), (f, k)
     # a series that is not 4-byte aligned is refused before any launch
     out = torch.empty(1000, dtype=torch.float32, device="cuda")
     lib = rb._lib.load()
