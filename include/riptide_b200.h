@@ -77,7 +77,8 @@ int rt_benchmark_ffa2(size_t rows, size_t cols, size_t loops, double* h_seconds)
 int rt_snr2(const float* d_in, size_t rows, size_t cols, const uint64_t* h_widths,
             size_t num_widths, float stdnoise, float* d_out, void* stream);
 
-/* downsample by a real factor 1 < f <= size; output floor(size / f) samples.
+/* downsample by a real factor 1 < f <= size; output floor(size / f) samples. d_in must be
+ * 4-byte aligned (any float array is); RT_EINVAL otherwise, before any launch.
  * Replaces python_bindings.cpp:163-177 (downsample.hpp:44-82). */
 int rt_downsample(const float* d_in, size_t size, double f, float* d_out, void* stream);
 
