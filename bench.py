@@ -772,7 +772,8 @@ def main():
     ap.add_argument("--no-grad", action="store_true",
                     help="skip the differentiable-search training step")
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--chunk-trials", type=int, default=32)
+    ap.add_argument("--chunk-trials", type=int, default=16,
+                    help="trials per SearchPipeline chunk in the end-to-end leg")
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--peaks", action="store_true")
