@@ -244,7 +244,7 @@ class SearchPipeline(object):
     overlap needs. Same outputs as ``BatchedSearch`` (every trial is searched independently).
     """
 
-    def __init__(self, lengths, tsamp, chunk_trials=64, period_min=1.0, period_max=30.0,
+    def __init__(self, lengths, tsamp, chunk_trials=16, period_min=1.0, period_max=30.0,
                  bins_min=240, bins_max=260, ducy_max=0.20, wtsp=1.5, deredden=True,
                  rmed_width=4.0, rmed_minpts=101, already_normalised=False, widths=None):
         self.lengths = np.ascontiguousarray(np.asarray(lengths, dtype=np.uint64).ravel())

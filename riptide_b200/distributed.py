@@ -125,7 +125,7 @@ def search_sharded(series, tsamp, rank, world, search=None, root=0, **search_kw)
     return gather_to_root(results, rank, world, root=root)
 
 
-def _pipeline_search(series, tsamp, chunk_trials=32, **search_kw):
+def _pipeline_search(series, tsamp, chunk_trials=16, **search_kw):
     from .batched import SearchPipeline
 
     pipe = SearchPipeline([s.size for s in series], tsamp, chunk_trials=chunk_trials,
