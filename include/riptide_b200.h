@@ -63,8 +63,10 @@ int rt_ffa2(const float* d_in, size_t rows, size_t cols, float* d_out, void* str
  * forbid cudaMalloc/cudaFree after start-up (they can block the whole device). No counterpart
  * in the reference. Scratch is a fixed 8 MiB array in this library, held by every GPU that
  * loads it: rows * cols <= 1048576 (cols <= 4096), else RT_EINVAL. The first call on a device
- * looks the array up (cudaGetSymbolAddress) and should come before any stream capture. Calls
- * share the array: calls that overlap on the GPU race and must not be issued. */
+ * looks the array up (cudaGetSymbolAddress) and should come before any stream capture; the
+ * address is kept for the life of the process, so cudaDeviceReset after that first call is
+ * not supported. Calls share the array: calls that overlap on the GPU race and must not be
+ * issued. */
 int rt_ffa2_noalloc(const float* d_in, size_t rows, size_t cols, float* d_out, void* stream);
 
 /* benchmark_ffa2: seconds per transform of a zero rows x cols block over `loops` runs
