@@ -251,15 +251,43 @@ __device__ void snr_rows_impl(const float* X, int xs, int nrows, int b, const Sn
             for (int q = 1; q < FastWidths10::NW; ++q) dm = (k == q) ? mx[q] : dm;
             orow[k] = __fdiv_rn(__fmaf_rn(S.hb[k], dm, -__fmul_rn(S.beta[k], sum)), stdnoise);
         }
-        // remaining widths: direct shared-memory reads
-        for (int k = S.nfast; k < S.nw; ++k) {
-            const int w = S.w[k];
-            float m = -INFINITY;
-            for (int i = i0; i < i1; ++i) m = fmaxf(m, __fsub_rn(cr[i + w], cr[i]));
+        // remaining widths (63 and 94 for bins_min 480), two at a time straight from shared
+        // memory: each phase's C[i] is loaded once for both widths, eight phases per step
+        for (int k = S.nfast; k < S.nw; k += 2) {
+            const bool two = k + 1 < S.nw;
+            const int w1 = S.w[k], w2 = two ? S.w[k + 1] : w1;
+            float m1 = -INFINITY, m2 = -INFINITY;
+            int i = i0;
+            for (; i + 8 <= i1; i += 8) {
+                float a[8], p[8], q[8];
 #pragma unroll
-            for (int o = TPR / 2; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(gmask, m, o, TPR));
-            if (t == 0)
-                orow[k] = __fdiv_rn(__fmaf_rn(S.hb[k], m, -__fmul_rn(S.beta[k], sum)), stdnoise);
+                for (int j = 0; j < 8; ++j) {
+                    a[j] = cr[i + j];
+                    p[j] = cr[i + j + w1];
+                    q[j] = cr[i + j + w2];
+                }
+#pragma unroll
+                for (int j = 0; j < 8; j += 2) {
+                    m1 = fmax3(m1, __fsub_rn(p[j], a[j]), __fsub_rn(p[j + 1], a[j + 1]));
+                    m2 = fmax3(m2, __fsub_rn(q[j], a[j]), __fsub_rn(q[j + 1], a[j + 1]));
+                }
+            }
+            for (; i < i1; ++i) {
+                const float a = cr[i];
+                m1 = fmaxf(m1, __fsub_rn(cr[i + w1], a));
+                m2 = fmaxf(m2, __fsub_rn(cr[i + w2], a));
+            }
+#pragma unroll
+            for (int o = TPR / 2; o > 0; o >>= 1) {
+                m1 = fmaxf(m1, __shfl_xor_sync(gmask, m1, o, TPR));
+                m2 = fmaxf(m2, __shfl_xor_sync(gmask, m2, o, TPR));
+            }
+            if (t == 0) {
+                orow[k] = __fdiv_rn(__fmaf_rn(S.hb[k], m1, -__fmul_rn(S.beta[k], sum)), stdnoise);
+                if (two)
+                    orow[k + 1] =
+                        __fdiv_rn(__fmaf_rn(S.hb[k + 1], m2, -__fmul_rn(S.beta[k + 1], sum)), stdnoise);
+            }
         }
         __syncwarp(gmask);  // cr is rewritten for the next profile
     }
