@@ -476,42 +476,61 @@ __device__ __forceinline__ void level_rows_generic(const RowOp* ops, int nrows,
     }
 }
 
-template <bool kGlobal>
+// Bins classes of a kernel instance: which unrolled level loops it contains. A kernel that
+// only ever sees b in [225, 288] (kBins256) or in [449, 544] (kBins512) leaves out the loops of
+// the other range (smaller code); kBinsAny has all of them. Any b still runs correctly in any
+// class (the generic loop), only slower.
+enum BinsClass { kBinsAny = 0, kBins256 = 1, kBins512 = 2 };
+
+RT_HD int bins_class(int bmin, int bmax)
+{
+    if (bmin >= 225 && bmax <= 288) return kBins256;
+    if (bmin >= 449 && bmax <= 544) return kBins512;
+    return kBinsAny;
+}
+
+template <bool kGlobal, int BC = kBinsAny>
 __device__ __forceinline__ void level_rows(const RowOp* ops, int nrows, const float* src,
                                            int sstride, float* dst, int stride, int b)
 {
+    constexpr bool k256 = BC != kBins512, k512 = BC != kBins256;
     if (!kGlobal && halo_mode(b)) {
         switch ((b + 63) >> 6) {
-            case 4: level_rows_pairs<4>(ops, nrows, src, sstride, dst, stride, b); return;
-            case 5: level_rows_pairs<5>(ops, nrows, src, sstride, dst, stride, b); return;
-            case 8: level_rows_pairs<8>(ops, nrows, src, sstride, dst, stride, b); return;
-            default: level_rows_pairs<9>(ops, nrows, src, sstride, dst, stride, b); return;
+            case 4: if constexpr (k256) { level_rows_pairs<4>(ops, nrows, src, sstride, dst, stride, b); return; } break;
+            case 5: if constexpr (k256) { level_rows_pairs<5>(ops, nrows, src, sstride, dst, stride, b); return; } break;
+            case 8: if constexpr (k512) { level_rows_pairs<8>(ops, nrows, src, sstride, dst, stride, b); return; } break;
+            default: if constexpr (k512) { level_rows_pairs<9>(ops, nrows, src, sstride, dst, stride, b); return; } break;
         }
     }
     const int nit = (b + 31) >> 5;
     switch (nit) {
-#define RT_NIT_CASE(N) \
-    case N: level_rows_unrolled<N, kGlobal>(ops, nrows, src, sstride, dst, stride, b); break;
+#define RT_NIT_CASE(N, K) \
+    case N: if constexpr (K) { level_rows_unrolled<N, kGlobal>(ops, nrows, src, sstride, dst, stride, b); return; } break;
         // bins 225-288 and 449-544 cover the usual searches (bins_min 240 / 480)
-        RT_NIT_CASE(8) RT_NIT_CASE(9) RT_NIT_CASE(15) RT_NIT_CASE(16) RT_NIT_CASE(17)
+        RT_NIT_CASE(8, k256) RT_NIT_CASE(9, k256) RT_NIT_CASE(15, k512) RT_NIT_CASE(16, k512)
+        RT_NIT_CASE(17, k512)
 #undef RT_NIT_CASE
-        default: level_rows_generic<kGlobal>(ops, nrows, src, sstride, dst, stride, b);
+        default: break;
     }
+    level_rows_generic<kGlobal>(ops, nrows, src, sstride, dst, stride, b);
 }
 
 // Level computed from source rows staged in shared memory (packed, stride b): same loop as
 // the global level, plain loads.
+template <int BC = kBinsAny>
 __device__ __forceinline__ void level_rows_staged(const RowOp* ops, int nrows, const float* src,
                                                   float* dst, int stride, int b)
 {
+    constexpr bool k256 = BC != kBins512, k512 = BC != kBins256;
     switch ((b + 31) >> 5) {
-        case 8: level_rows_unrolled<8, false>(ops, nrows, src, b, dst, stride, b); break;
-        case 9: level_rows_unrolled<9, false>(ops, nrows, src, b, dst, stride, b); break;
-        case 15: level_rows_unrolled<15, false>(ops, nrows, src, b, dst, stride, b); break;
-        case 16: level_rows_unrolled<16, false>(ops, nrows, src, b, dst, stride, b); break;
-        case 17: level_rows_unrolled<17, false>(ops, nrows, src, b, dst, stride, b); break;
-        default: level_rows_generic<false>(ops, nrows, src, b, dst, stride, b);
+        case 8: if constexpr (k256) { level_rows_unrolled<8, false>(ops, nrows, src, b, dst, stride, b); return; } break;
+        case 9: if constexpr (k256) { level_rows_unrolled<9, false>(ops, nrows, src, b, dst, stride, b); return; } break;
+        case 15: if constexpr (k512) { level_rows_unrolled<15, false>(ops, nrows, src, b, dst, stride, b); return; } break;
+        case 16: if constexpr (k512) { level_rows_unrolled<16, false>(ops, nrows, src, b, dst, stride, b); return; } break;
+        case 17: if constexpr (k512) { level_rows_unrolled<17, false>(ops, nrows, src, b, dst, stride, b); return; } break;
+        default: break;
     }
+    level_rows_generic<false>(ops, nrows, src, b, dst, stride, b);
 }
 
 // Where a job's levels read and write outside the two level buffers.
@@ -532,6 +551,7 @@ struct LevelIO {
 // `stride`, row i of the buffer = root output row lo + i), or in global memory if
 // io.root_dst is given. `ops` has room for the largest level. Returns false if the wait for
 // staged rows ran out.
+template <int BC = kBinsAny>
 __device__ inline bool run_job_levels(const JobTree& T, int b, float* buf0, float* buf1,
                                       int stride, RowOp* ops, const LevelIO& io)
 {
@@ -551,13 +571,13 @@ __device__ inline bool run_job_levels(const JobTree& T, int b, float* buf0, floa
         // one call site per level loop kind (the loops are large once unrolled)
         const bool first = d == T.depth;
         if (first && !io.staged) {
-            level_rows<true>(lops, T.level_rows[d], io.src, io.src_stride, dst, dstride, b);
+            level_rows<true, BC>(lops, T.level_rows[d], io.src, io.src_stride, dst, dstride, b);
         } else if (first && !io.staged_rows) {
-            level_rows_staged(lops, T.level_rows[d], io.staged, dst, dstride, b);
+            level_rows_staged<BC>(lops, T.level_rows[d], io.staged, dst, dstride, b);
         } else {
             // shared-memory source: level d + 1, or the staged rows of level G's children
             const float* from = first ? io.staged : ((d & 1) ? buf0 : buf1);
-            level_rows<false>(lops, T.level_rows[d], from, stride, dst, dstride, b);
+            level_rows<false, BC>(lops, T.level_rows[d], from, stride, dst, dstride, b);
         }
         cta_sync();
     }
