@@ -494,24 +494,46 @@ __device__ __forceinline__ void level_rows(const RowOp* ops, int nrows, const fl
                                            int sstride, float* dst, int stride, int b)
 {
     constexpr bool k256 = BC != kBins512, k512 = BC != kBins256;
+    // each case runs its unrolled loop and returns when the class holds it, else falls
+    // through to the generic loop below
+#define RT_PAIRS_CASE(N, K)                                                   \
+    case N:                                                                   \
+        if constexpr (K) {                                                    \
+            level_rows_pairs<N>(ops, nrows, src, sstride, dst, stride, b);    \
+            return;                                                           \
+        }                                                                     \
+        break;
     if (!kGlobal && halo_mode(b)) {
         switch ((b + 63) >> 6) {
-            case 4: if constexpr (k256) { level_rows_pairs<4>(ops, nrows, src, sstride, dst, stride, b); return; } break;
-            case 5: if constexpr (k256) { level_rows_pairs<5>(ops, nrows, src, sstride, dst, stride, b); return; } break;
-            case 8: if constexpr (k512) { level_rows_pairs<8>(ops, nrows, src, sstride, dst, stride, b); return; } break;
-            default: if constexpr (k512) { level_rows_pairs<9>(ops, nrows, src, sstride, dst, stride, b); return; } break;
+            RT_PAIRS_CASE(4, k256)
+            RT_PAIRS_CASE(5, k256)
+            RT_PAIRS_CASE(8, k512)
+            default:  // 9
+                if constexpr (k512) {
+                    level_rows_pairs<9>(ops, nrows, src, sstride, dst, stride, b);
+                    return;
+                }
+                break;
         }
     }
-    const int nit = (b + 31) >> 5;
-    switch (nit) {
-#define RT_NIT_CASE(N, K) \
-    case N: if constexpr (K) { level_rows_unrolled<N, kGlobal>(ops, nrows, src, sstride, dst, stride, b); return; } break;
+#undef RT_PAIRS_CASE
+#define RT_NIT_CASE(N, K)                                                              \
+    case N:                                                                            \
+        if constexpr (K) {                                                             \
+            level_rows_unrolled<N, kGlobal>(ops, nrows, src, sstride, dst, stride, b); \
+            return;                                                                    \
+        }                                                                              \
+        break;
+    switch ((b + 31) >> 5) {
         // bins 225-288 and 449-544 cover the usual searches (bins_min 240 / 480)
-        RT_NIT_CASE(8, k256) RT_NIT_CASE(9, k256) RT_NIT_CASE(15, k512) RT_NIT_CASE(16, k512)
+        RT_NIT_CASE(8, k256)
+        RT_NIT_CASE(9, k256)
+        RT_NIT_CASE(15, k512)
+        RT_NIT_CASE(16, k512)
         RT_NIT_CASE(17, k512)
-#undef RT_NIT_CASE
         default: break;
     }
+#undef RT_NIT_CASE
     level_rows_generic<kGlobal>(ops, nrows, src, sstride, dst, stride, b);
 }
 
@@ -522,14 +544,22 @@ __device__ __forceinline__ void level_rows_staged(const RowOp* ops, int nrows, c
                                                   float* dst, int stride, int b)
 {
     constexpr bool k256 = BC != kBins512, k512 = BC != kBins256;
+#define RT_NIT_CASE(N, K)                                                         \
+    case N:                                                                       \
+        if constexpr (K) {                                                        \
+            level_rows_unrolled<N, false>(ops, nrows, src, b, dst, stride, b);    \
+            return;                                                               \
+        }                                                                         \
+        break;
     switch ((b + 31) >> 5) {
-        case 8: if constexpr (k256) { level_rows_unrolled<8, false>(ops, nrows, src, b, dst, stride, b); return; } break;
-        case 9: if constexpr (k256) { level_rows_unrolled<9, false>(ops, nrows, src, b, dst, stride, b); return; } break;
-        case 15: if constexpr (k512) { level_rows_unrolled<15, false>(ops, nrows, src, b, dst, stride, b); return; } break;
-        case 16: if constexpr (k512) { level_rows_unrolled<16, false>(ops, nrows, src, b, dst, stride, b); return; } break;
-        case 17: if constexpr (k512) { level_rows_unrolled<17, false>(ops, nrows, src, b, dst, stride, b); return; } break;
+        RT_NIT_CASE(8, k256)
+        RT_NIT_CASE(9, k256)
+        RT_NIT_CASE(15, k512)
+        RT_NIT_CASE(16, k512)
+        RT_NIT_CASE(17, k512)
         default: break;
     }
+#undef RT_NIT_CASE
     level_rows_generic<false>(ops, nrows, src, b, dst, stride, b);
 }
 
