@@ -444,7 +444,10 @@ __device__ __forceinline__ void level_rows_pairs(const RowOp* ops, int nrows,
                 out[64 * j + 32] = s1;
             } else {
                 if (c < b) out[64 * j] = __fadd_rn(H[64 * j], p0[64 * j]);
-                if (c + 32 < b) out[64 * j + 32] = __fadd_rn(H[64 * j + 32], p1[64 * j + 32]);
+                // the last chunk's second half (columns from 64 (NIT2 - 1) + 32) is empty for
+                // every b of the 5- and 9-chunk ranges (b <= 288 and b <= 544)
+                constexpr bool kHalf2 = NIT2 != 5 && NIT2 != 9;
+                if (kHalf2 && c + 32 < b) out[64 * j + 32] = __fadd_rn(H[64 * j + 32], p1[64 * j + 32]);
             }
         }
     }
